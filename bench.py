@@ -1,0 +1,535 @@
+#!/usr/bin/env python
+"""Benchmark of the batched Kronecker matvec on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config 1..5] [--mode atomic|segmented]
+
+Default workload (the overlapping-output case the headline metric is quoted
+on): kronmult3_xbatched, d=3, n=8, FP64; an element grid of 8192 elements,
+each coupled to itself and 15 distinct random neighbours -> 131072 entries,
+Ylist[k] = element i, Xlist[k] = element j; every A_l is a pointer into a
+pool of 64 random 8x8 matrices per dimension, N(0,1)/sqrt(8); X ~ U(-1,1).
+All data is synthetic (seeded numpy PCG64); the reference publishes no
+dataset.  Other --config values are measurement cases for the design notes
+(1: kronmult6_batched n=4 batch 512; 3: precision sweep n in {4,6} batch
+4096; 4: uneven batch of 20000 entries; 5: d=6 n=8 batch 1024 with shared
+outputs).
+
+One step = one call of the library over the whole batch with inputs resident
+in HBM.  Steps are timed one by one with CUDA events on the launching stream
+and L2 is flushed (256 MB write) between timed steps, outside the events.
+Multi-GPU: replicas (each rank runs the whole workload; no collective on the
+data path), barrier + max over ranks.
+
+Prints ONE JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SEED = 20261203
+METRIC = "kronmult GFLOP/s + HBM GB/s vs roofline; FP32/split vs FP64 speedup at stated err"
+
+
+# ---------------------------------------------------------------- workloads
+class Workload:
+    name = ""
+    dtype = "f64"
+    launches_per_step = 1
+
+    def flops(self) -> float:
+        raise NotImplementedError
+
+    def alg_bytes(self) -> float:
+        raise NotImplementedError
+
+
+class XbatchedOverlap(Workload):
+    """kronmult3_xbatched d=3 n=8, 8192 elements x 16 couplings (131072 entries)."""
+
+    def __init__(self, nelem=8192, ncoup=16, d=3, n=8, npool=64, seed=SEED + 1):
+        rng = np.random.default_rng(seed)
+        self.d, self.n, self.npool, self.nelem = d, n, npool, nelem
+        self.L = n ** d
+        self.Apool = rng.standard_normal(n * n * npool * d) / np.sqrt(n)
+        ylist = np.repeat(np.arange(nelem), ncoup)
+        xlist = np.empty(nelem * ncoup, dtype=np.int64)
+        for i in range(nelem):
+            nb = rng.choice(nelem - 1, size=ncoup - 1, replace=False)
+            nb = nb + (nb >= i)  # skip self
+            xlist[i * ncoup] = i
+            xlist[i * ncoup + 1:(i + 1) * ncoup] = nb
+        self.ylist, self.xlist = ylist, xlist
+        self.batch = len(ylist)
+        self.aidx = rng.integers(0, npool, size=(self.batch, d))
+        self.X = rng.uniform(-1, 1, self.L * nelem)
+        self.name = (f"kronmult{d}_xbatched n={n} FP64, {nelem} elements x {ncoup} couplings "
+                     f"= {self.batch} entries, A pool {npool}/dim")
+
+    def flops(self):
+        return float(self.batch) * 2 * self.d * self.n ** (self.d + 1)
+
+    def alg_bytes(self):
+        # distinct X read once, distinct Y read+written once, A pool once
+        return 8.0 * (self.L * self.nelem + 2 * self.L * self.nelem + self.Apool.size)
+
+    def a_offsets(self):
+        n, d, npool = self.n, self.d, self.npool
+        l = np.arange(d)[None, :]
+        return (n * n * (l * npool + self.aidx)).reshape(-1)
+
+    # -- GPU
+    def setup(self, torch, kb, mode):
+        dev = torch.device("cuda")
+        self.kb = kb
+        self.mode = mode
+        self.dA = torch.from_numpy(self.Apool).to(dev)
+        self.dX = torch.from_numpy(self.X).to(dev)
+        self.dY = torch.zeros(self.L * self.nelem, dtype=torch.float64, device=dev)
+        self.pA = (self.dA.data_ptr() + 8 * torch.from_numpy(self.a_offsets())).to(dev)
+        self.pX = (self.dX.data_ptr() + 8 * self.L * torch.from_numpy(self.xlist)).to(dev)
+        self.pY = (self.dY.data_ptr() + 8 * self.L * torch.from_numpy(self.ylist)).to(dev)
+        self.seg = kb.Segments(self.pY) if mode == "segmented" else None
+        # e2e: pinned host copies of every input of the call
+        self.h = {k: v.cpu().pin_memory() for k, v in
+                  dict(A=self.dA, X=self.dX, Y=self.dY, pA=self.pA, pX=self.pX,
+                       pY=self.pY).items()}
+        self.hYout = torch.empty_like(self.h["Y"]).pin_memory()
+        self.h2d_bytes = sum(v.numel() * v.element_size() for v in self.h.values())
+        self.d2h_bytes = self.hYout.numel() * 8
+
+    def step(self):
+        if self.seg is not None:
+            self.kb.kronmult_xbatched_segmented(self.d, self.n, self.pA, self.n, self.pX,
+                                                self.pY, self.seg)
+        else:
+            self.kb.kronmult_xbatched(self.d, self.n, self.pA, self.n, self.pX, self.pY)
+
+    def e2e_step(self):
+        # host -> device (pinned, async), the library call, device -> host of Y
+        self.dA.copy_(self.h["A"], non_blocking=True)
+        self.dX.copy_(self.h["X"], non_blocking=True)
+        self.dY.copy_(self.h["Y"], non_blocking=True)
+        self.pA.copy_(self.h["pA"], non_blocking=True)
+        self.pX.copy_(self.h["pX"], non_blocking=True)
+        self.pY.copy_(self.h["pY"], non_blocking=True)
+        self.step()
+        self.hYout.copy_(self.dY, non_blocking=True)
+
+    # -- CPU reference (OpenMP build of the reference's own kronmult3_xbatched)
+    def cpu_setup(self, sample_entries):
+        self.cs = min(self.batch, sample_entries)
+        self.cX = self.X.copy()
+        self.cY = np.zeros(self.L * self.nelem)
+        self.cW = np.zeros(self.L * self.cs)
+        base_a = self.Apool.ctypes.data
+        self.c_ap = (base_a + 8 * self.a_offsets()[: self.cs * self.d]).astype(np.uint64)
+        self.c_xp = (self.cX.ctypes.data + 8 * self.L * self.xlist[: self.cs]).astype(np.uint64)
+        self.c_yp = (self.cY.ctypes.data + 8 * self.L * self.ylist[: self.cs]).astype(np.uint64)
+        self.c_wp = (self.cW.ctypes.data + 8 * self.L * np.arange(self.cs)).astype(np.uint64)
+        return self.cs
+
+    def cpu_step(self, ref):
+        ref.kronmult_xbatched(self.d, self.n, self.c_ap, self.n, self.c_xp, self.c_yp, self.c_wp,
+                              0)
+
+    def cpu_flops(self):
+        return float(self.cs) * 2 * self.d * self.n ** (self.d + 1)
+
+
+class BatchedSquare(Workload):
+    """kronmult{d}_batched (distinct outputs), FP64 / FP32 / split."""
+
+    def __init__(self, d=6, n=4, batch=512, precision="f64", dist="uniform", seed=SEED):
+        rng = np.random.default_rng(seed)
+        self.d, self.n, self.batch, self.precision = d, n, batch, precision
+        self.L = n ** d
+        if dist == "uniform":
+            self.A = rng.uniform(-1, 1, n * n * d * batch)
+        else:
+            self.A = rng.standard_normal(n * n * d * batch) / np.sqrt(n)
+        self.X = rng.uniform(-1, 1, self.L * batch)
+        self.dtype = {"f64": "f64", "f32": "f32", "split": "f64 storage, hi+lo f32 math"}[
+            precision]
+        self.name = f"kronmult{d}_batched n={n} batch={batch} {precision}"
+
+    def esize(self):
+        return 4 if self.precision == "f32" else 8
+
+    def flops(self):
+        return float(self.batch) * 2 * self.d * self.n ** (self.d + 1)
+
+    def alg_bytes(self):
+        return self.esize() * float(self.batch) * (3 * self.L + self.d * self.n * self.n)
+
+    def setup(self, torch, kb, mode):
+        dev = torch.device("cuda")
+        dt = torch.float32 if self.precision == "f32" else torch.float64
+        self.kb = kb
+        self.dA = torch.from_numpy(self.A).to(dev, dt)
+        self.dX = torch.from_numpy(self.X).to(dev, dt)
+        self.dY = torch.zeros(self.L * self.batch, dtype=dt, device=dev)
+        need = kb.lib().kron_batched_workspace_bytes(self.d, self.n, self.batch)
+        self.dW = torch.empty(max(1, need // 8), dtype=dt, device=dev) if need else None
+        self.launches_per_step = 2 if need else 1
+        self.h = {k: v.cpu().pin_memory() for k, v in dict(A=self.dA, X=self.dX,
+                                                          Y=self.dY).items()}
+        self.hYout = torch.empty_like(self.h["Y"]).pin_memory()
+        self.h2d_bytes = sum(v.numel() * v.element_size() for v in self.h.values())
+        self.d2h_bytes = self.hYout.numel() * self.hYout.element_size()
+
+    def step(self):
+        kb = self.kb
+        if self.precision == "f32":
+            kb.kronmult_batched_f32(self.d, self.n, self.dA, self.dX, self.dY, self.dW)
+        elif self.precision == "split":
+            kb.kronmult_batched_split(self.d, self.n, self.dA, self.dX, self.dY, self.dW)
+        else:
+            kb.kronmult_batched(self.d, self.n, self.dA, self.dX, self.dY, self.dW)
+
+    def e2e_step(self):
+        self.dA.copy_(self.h["A"], non_blocking=True)
+        self.dX.copy_(self.h["X"], non_blocking=True)
+        self.dY.copy_(self.h["Y"], non_blocking=True)
+        self.step()
+        self.hYout.copy_(self.dY, non_blocking=True)
+
+    def cpu_setup(self, sample_entries):
+        self.cs = min(self.batch, sample_entries)
+        self.cA = self.A[: self.cs * self.d * self.n * self.n].copy()
+        self.cX = self.X[: self.cs * self.L].copy()
+        self.cY = np.zeros(self.cs * self.L)
+        self.cW = np.zeros(self.cs * self.L)
+        return self.cs
+
+    def cpu_step(self, ref):
+        Xc = self.cX.copy()  # the reference clobbers X
+        ref.kronmult_batched(self.d, self.n, self.cA, Xc, self.cY, self.cW)
+
+    def cpu_flops(self):
+        return float(self.cs) * 2 * self.d * self.n ** (self.d + 1)
+
+
+def make_workload(cfg, precision):
+    if cfg == 1:
+        return BatchedSquare(6, 4, 512, "f64", "uniform")
+    if cfg == 2:
+        return XbatchedOverlap()
+    if cfg == 3:
+        n = int(os.environ.get("KRON_BENCH_N", "4"))
+        return BatchedSquare(6, n, 4096, precision, "normal")
+    raise SystemExit(f"--config {cfg} not available in this bench")
+
+
+# ---------------------------------------------------------------- helpers
+def read_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def read_profile_traffic(config):
+    """Per-launch DRAM traffic of the dominant kernel from the committed ncu
+    summary (profiles/*.md line `traffic_bytes_per_launch[cfgN]: <bytes>`)."""
+    import glob
+    import re
+
+    for p in glob.glob(os.path.join(ROOT, "profiles", "*.md")):
+        with open(p) as f:
+            for line in f:
+                m = re.match(rf"\s*traffic_bytes_per_launch\[cfg{config}\]:\s*([0-9.eE+]+)", line)
+                if m:
+                    return float(m.group(1)), os.path.relpath(p, ROOT)
+    return None, None
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.proc = None
+        self.dev = device_index
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={device_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args, world, rank):
+    """The reference's own CPU (OpenMP) implementation of the same workload,
+    on the host cores: oracle/_ref (compiled from the reference sources) when
+    present, else the oracle's C port."""
+    if rank != 0:
+        return
+    import oracle
+
+    wl = make_workload(args.config, args.precision)
+    if oracle.Reference.available("recur"):
+        ref = oracle.Reference("recur")
+        kind = "reference"
+        cores = ref.max_threads()
+    else:
+        raise SystemExit(json.dumps({"impl": "reference",
+                                     "unavailable": "oracle/_ref not built on this machine"}))
+    sample = wl.cpu_setup(args.cpu_sample)
+    for _ in range(args.warmup):
+        wl.cpu_step(ref)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        wl.cpu_step(ref)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = wl.cpu_flops() * len(times) / tot / 1e9
+    line = {"metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s",
+            "impl": "reference", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * tot / len(times), 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wl.name, "sample_entries": sample},
+            "cpu_baseline": {"value": round(value, 3), "unit": "GFLOP/s", "cores": cores,
+                             "kind": kind,
+                             "sample": f"{sample} of {wl.batch} entries per step, "
+                                       f"OpenMP {cores} threads, recursive variant"},
+            "e2e": {"value": round(value, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, world, rank, local):
+    import torch
+
+    import kronmult_b200 as kb
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    kb.lib()
+    wl = make_workload(args.config, args.precision)
+    wl.setup(torch, kb, args.mode)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        wl.step()
+        flush.zero_()
+    barrier()
+    clock = ClockSampler(local) if rank == 0 else None
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for i in range(args.steps):
+        starts[i].record()
+        wl.step()
+        ends[i].record()
+        flush.zero_()
+    barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    tot_ms = sum(step_ms)
+
+    # e2e through the public API with pinned host buffers
+    for _ in range(max(1, args.warmup // 2)):
+        wl.e2e_step()
+    barrier()
+    e_s = torch.cuda.Event(enable_timing=True)
+    e_e = torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(1, min(args.steps, 10))
+    e_s.record()
+    for _ in range(e2e_steps):
+        wl.e2e_step()
+    e_e.record()
+    barrier()
+    e2e_ms = e_s.elapsed_time(e_e)
+    clocks = clock.stop() if clock else None
+
+    if dist is not None:
+        t = torch.tensor([tot_ms, e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms, e2e_ms = t.tolist()
+
+    # CPU baseline (rank 0, N=1 only): the reference's OpenMP build, bounded sample
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(wl, args)
+
+    if rank == 0:
+        peaks, peak_src = read_peaks()
+        flops = wl.flops()
+        sec = tot_ms / 1e3
+        value = world * flops * args.steps / sec / 1e9
+        gbs = wl.alg_bytes() * args.steps / sec / 1e9
+        per_launch_s = sec / (args.steps * wl.launches_per_step)
+        traffic, tsrc = read_profile_traffic(args.config)
+        if args.config == 2 or args.config == 5:
+            fp64 = measure_fp64_peak(torch)
+            roof = {"bound": "tensor", "achieved": round(flops / wl.launches_per_step /
+                                                         per_launch_s / 1e12, 3),
+                    "peak": round(fp64, 3), "unit": "TFLOP/s",
+                    "frac": round(flops / wl.launches_per_step / per_launch_s / 1e12 / fp64, 4),
+                    "traffic": traffic,
+                    "peak_source": "FP64 DGEMM 8192^3 (cuBLAS, tensor-core FP64) measured in "
+                                   "this run; MEASURED_PEAKS.json has no FP64 figure",
+                    "hbm_gbs_achieved": round(gbs, 1),
+                    "hbm_frac": round(gbs / peaks["hbm_gbs"], 4)}
+        else:
+            roof = {"bound": "hbm", "achieved": round(wl.alg_bytes() / wl.launches_per_step /
+                                                      per_launch_s / 1e9, 1),
+                    "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": round(wl.alg_bytes() / wl.launches_per_step / per_launch_s / 1e9 /
+                                  peaks["hbm_gbs"], 4),
+                    "traffic": traffic, "peak_source": f"MEASURED_PEAKS.json ({peak_src})"}
+        if tsrc:
+            roof["traffic_source"] = tsrc
+        line = {"metric": METRIC, "value": round(value, 2), "unit": "GFLOP/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(tot_ms / args.steps, 5), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": wl.dtype,
+                "data": "synthetic (seeded PCG64; no public dataset exists)",
+                "config": {"workload": wl.name, "mode": args.mode,
+                           "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                           "l2": "256 MB flush between timed steps (outside the events)",
+                           "alg_bytes_per_step": wl.alg_bytes(), "flops_per_step": flops},
+                "hbm_gbs": round(world * gbs, 1),
+                "roofline": roof,
+                "cpu_baseline": cpu,
+                "e2e": {"value": round(world * flops * e2e_steps / (e2e_ms / 1e3) / 1e9, 2),
+                        "unit": "GFLOP/s", "h2d_bytes_per_step": wl.h2d_bytes,
+                        "d2h_bytes_per_step": wl.d2h_bytes,
+                        "ms_per_step": round(e2e_ms / e2e_steps, 4)},
+                "gpu_launches": args.steps * wl.launches_per_step,
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def measure_fp64_peak(torch):
+    """FP64 throughput of cuBLAS DGEMM 8192^3 (best of 5), TFLOP/s."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def cpu_baseline(wl, args):
+    import oracle
+
+    if not oracle.Reference.available("recur"):
+        return None
+    ref = oracle.Reference("recur")
+    sample = wl.cpu_setup(args.cpu_sample)
+    wl.cpu_step(ref)
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        wl.cpu_step(ref)
+        n += 1
+        if time.perf_counter() - t0 > args.cpu_seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": round(wl.cpu_flops() * n / dt / 1e9, 3), "unit": "GFLOP/s",
+            "cores": ref.max_threads(), "kind": "reference",
+            "sample": f"{sample} of {wl.batch} entries x {n} repetitions "
+                      f"({dt:.1f} s), reference OpenMP build, recursive variant"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--mode", default="atomic", choices=["atomic", "segmented"])
+    ap.add_argument("--precision", default="f64", choices=["f64", "f32", "split"])
+    ap.add_argument("--cpu-sample", type=int, default=1 << 30)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,341 @@
+/*
+ * kronmult_b200 -- batched Kronecker matrix-vector products on NVIDIA B200
+ * (sm_100a).  For every batch entry k:
+ *
+ *     Y(:,k) += kron(A_1(k), ..., A_d(k)) * X(:,k),      d = 1..6
+ *
+ * with A_d's index fastest in X and Y and every matrix column major.
+ *
+ * Two layers are exported from libkronmult_b200.so:
+ *
+ *  1. The reference KRONMULT host entry points with their exact C++
+ *     signatures (C++ linkage, so existing C++ callers relink unchanged).
+ *     They launch on the legacy default stream, return nothing, and record
+ *     their status for kron_get_last_status() -- the reference has no error
+ *     return at all.
+ *
+ *  2. An extern "C" twin for each, suffixed _async, that takes an explicit
+ *     stream and returns a kron_status_t; plus extensions with no reference
+ *     counterpart (FP32 / split precision, deterministic segmented
+ *     accumulation, per-entry-shape vbatched, workspace queries).
+ *
+ * Every pointer argument (data, pointer arrays, ld arrays) is a DEVICE
+ * pointer, as in the reference GPU build (test_kronmult6_xbatched.cpp:243-271),
+ * unless a comment says "host".  All calls are asynchronous on their stream.
+ *
+ * Differences from the reference that callers may observe (all are
+ * strict relaxations):
+ *   - X is never modified (the reference batched/pbatched clobber X and W,
+ *     kronmult6_batched.hpp:10);
+ *   - W is accepted but only used for vectors too large for on-chip
+ *     storage; its contents are never relied upon;
+ *   - entries whose outputs alias are summed on the GPU in an unspecified
+ *     order in the default (atomic) mode, like the reference's atomicAdd.
+ */
+#ifndef KRONMULT_B200_H
+#define KRONMULT_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same type as cudaStream_t; NULL is the legacy default stream. */
+typedef struct CUstream_st *kron_stream_t;
+
+typedef enum kron_status
+{
+  KRON_SUCCESS             = 0,
+  KRON_ERROR_INVALID_VALUE = 1, /* bad size, null pointer, d out of 1..6 */
+  KRON_ERROR_WORKSPACE     = 2, /* the W provided is too small for the path */
+  KRON_ERROR_LAUNCH        = 3, /* a CUDA runtime / launch error */
+  KRON_ERROR_NOT_SUPPORTED = 4, /* combination not implemented */
+  KRON_ERROR_ALLOC         = 5, /* device or host allocation failed */
+  KRON_ERROR_INTERNAL      = 6
+} kron_status_t;
+
+const char *kron_status_string(int status);
+
+/* Status of the last reference-signature (void) call made on this host
+ * thread; KRON_SUCCESS if none failed.  Reading it does not reset it. */
+int kron_get_last_status(void);
+void kron_clear_last_status(void);
+
+/* Library version "major.minor.patch". */
+const char *kron_version(void);
+
+/* ------------------------------------------------------------------------
+ * batched: A is (n,n,d,batchCount) contiguous; X, Y, W are (n^d, batchCount).
+ * Replaces kronmult{d}_batched (kronmult6_batched.cpp:4-18).  Every entry
+ * writes its own Y column.  W may be NULL when n^d doubles fit on chip
+ * (kron_batched_workspace_bytes() returns 0 then).
+ * ---------------------------------------------------------------------- */
+int kronmult1_batched_async(int n, double const Aarray_[], double Xarray_[], double Yarray_[],
+                            double Warray_[], int batchCount, kron_stream_t stream);
+int kronmult2_batched_async(int n, double const Aarray_[], double Xarray_[], double Yarray_[],
+                            double Warray_[], int batchCount, kron_stream_t stream);
+int kronmult3_batched_async(int n, double const Aarray_[], double Xarray_[], double Yarray_[],
+                            double Warray_[], int batchCount, kron_stream_t stream);
+int kronmult4_batched_async(int n, double const Aarray_[], double Xarray_[], double Yarray_[],
+                            double Warray_[], int batchCount, kron_stream_t stream);
+int kronmult5_batched_async(int n, double const Aarray_[], double Xarray_[], double Yarray_[],
+                            double Warray_[], int batchCount, kron_stream_t stream);
+int kronmult6_batched_async(int n, double const Aarray_[], double Xarray_[], double Yarray_[],
+                            double Warray_[], int batchCount, kron_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * pbatched: A as in batched; X, Y, W are arrays of batchCount device
+ * pointers to n^d doubles.  Y pointers may alias (outputs are then summed).
+ * Replaces kronmult{d}_pbatched (kronmult6_pbatched.cpp:4-19).
+ * ---------------------------------------------------------------------- */
+int kronmult1_pbatched_async(int n, double const Aarray_[], double *Xarray_[], double *Yarray_[],
+                             double *Warray_[], int batchCount, kron_stream_t stream);
+int kronmult2_pbatched_async(int n, double const Aarray_[], double *Xarray_[], double *Yarray_[],
+                             double *Warray_[], int batchCount, kron_stream_t stream);
+int kronmult3_pbatched_async(int n, double const Aarray_[], double *Xarray_[], double *Yarray_[],
+                             double *Warray_[], int batchCount, kron_stream_t stream);
+int kronmult4_pbatched_async(int n, double const Aarray_[], double *Xarray_[], double *Yarray_[],
+                             double *Warray_[], int batchCount, kron_stream_t stream);
+int kronmult5_pbatched_async(int n, double const Aarray_[], double *Xarray_[], double *Yarray_[],
+                             double *Warray_[], int batchCount, kron_stream_t stream);
+int kronmult6_pbatched_async(int n, double const Aarray_[], double *Xarray_[], double *Yarray_[],
+                             double *Warray_[], int batchCount, kron_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * xbatched: Aarray_ holds d*batchCount device pointers, entry k's A_l at
+ * Aarray_[(l-1) + (k-1)*d], each n x n with leading dimension lda >= n.
+ * X, Y, W are pointer arrays; Y may alias.  subbatchCount <= 0 means the
+ * reference default max(1, batchCount/2); it bounds how many W pointers
+ * are used (2*subbatchCount, each n^d doubles) when W is needed at all.
+ * Replaces kronmult{d}_xbatched (kronmult6_xbatched.cpp:4-28,
+ * kronmult_xbatched.hpp:17-162).
+ * ---------------------------------------------------------------------- */
+int kronmult1_xbatched_async(int n, double const *const Aarray_[], int lda, double *Xarray_[],
+                             double *Yarray_[], double *Warray_[], int batchCount,
+                             int subbatchCount, kron_stream_t stream);
+int kronmult2_xbatched_async(int n, double const *const Aarray_[], int lda, double *Xarray_[],
+                             double *Yarray_[], double *Warray_[], int batchCount,
+                             int subbatchCount, kron_stream_t stream);
+int kronmult3_xbatched_async(int n, double const *const Aarray_[], int lda, double *Xarray_[],
+                             double *Yarray_[], double *Warray_[], int batchCount,
+                             int subbatchCount, kron_stream_t stream);
+int kronmult4_xbatched_async(int n, double const *const Aarray_[], int lda, double *Xarray_[],
+                             double *Yarray_[], double *Warray_[], int batchCount,
+                             int subbatchCount, kron_stream_t stream);
+int kronmult5_xbatched_async(int n, double const *const Aarray_[], int lda, double *Xarray_[],
+                             double *Yarray_[], double *Warray_[], int batchCount,
+                             int subbatchCount, kron_stream_t stream);
+int kronmult6_xbatched_async(int n, double const *const Aarray_[], int lda, double *Xarray_[],
+                             double *Yarray_[], double *Warray_[], int batchCount,
+                             int subbatchCount, kron_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * vbatched: rectangular A_l (m_l x n_l, leading dimension m_l), the same
+ * shapes for every entry; Aarray_ as in xbatched; X has prod(n_l), Y has
+ * prod(m_l) entries per vector; W is one flat device buffer of
+ * Wcapacity_bytes (may be 0 / NULL when everything fits on chip;
+ * kron_vbatched_workspace_bytes() gives the exact need -- the reference's
+ * own sizing is too small for Alg. 993 on rectangular shapes,
+ * kronmult_vbatched.hpp:107-135).  The reference only has the kernel
+ * templates kronmult{d}_vbatched<T> (kronmult6_vbatched.hpp:10-34); these
+ * are the host entry points it lacks.
+ * ---------------------------------------------------------------------- */
+int kronmult1_vbatched_async(int m1, int n1, double const *const Aarray_[], double *pX_[],
+                             double *pY_[], double *W_, size_t Wcapacity_bytes, int batchCount,
+                             kron_stream_t stream);
+int kronmult2_vbatched_async(int m1, int n1, int m2, int n2, double const *const Aarray_[],
+                             double *pX_[], double *pY_[], double *W_, size_t Wcapacity_bytes,
+                             int batchCount, kron_stream_t stream);
+int kronmult3_vbatched_async(int m1, int n1, int m2, int n2, int m3, int n3,
+                             double const *const Aarray_[], double *pX_[], double *pY_[],
+                             double *W_, size_t Wcapacity_bytes, int batchCount,
+                             kron_stream_t stream);
+int kronmult4_vbatched_async(int m1, int n1, int m2, int n2, int m3, int n3, int m4, int n4,
+                             double const *const Aarray_[], double *pX_[], double *pY_[],
+                             double *W_, size_t Wcapacity_bytes, int batchCount,
+                             kron_stream_t stream);
+int kronmult5_vbatched_async(int m1, int n1, int m2, int n2, int m3, int n3, int m4, int n4,
+                             int m5, int n5, double const *const Aarray_[], double *pX_[],
+                             double *pY_[], double *W_, size_t Wcapacity_bytes, int batchCount,
+                             kron_stream_t stream);
+int kronmult6_vbatched_async(int m1, int n1, int m2, int n2, int m3, int n3, int m4, int n4,
+                             int m5, int n5, int m6, int n6, double const *const Aarray_[],
+                             double *pX_[], double *pY_[], double *W_, size_t Wcapacity_bytes,
+                             int batchCount, kron_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * kgemm_{nn,nt,tt}_batched: C_k = alpha op(A_k) op(B_k) + beta C_k with
+ * op(A) = A (nn, nt) or A^T (tt), op(B) = B (nn) or B^T (nt, tt); mm x kk
+ * times kk x nn; pointer arrays and per-entry leading dimensions.
+ * beta == 1 accumulates atomically (C pointers may alias), beta == 0 never
+ * reads C.  Replaces kgemm_{nn,nt,tt}_batched (kgemm_nn_batched.cpp:5-25).
+ * ---------------------------------------------------------------------- */
+int kgemm_nn_batched_async(int mm, int nn, int kk, double alpha, double *const Aarray_[],
+                           int const ldAarray_[], double *const Barray_[], int const ldBarray_[],
+                           double beta, double *const Carray_[], int const ldCarray_[],
+                           int batchCount, kron_stream_t stream);
+int kgemm_nt_batched_async(int mm, int nn, int kk, double alpha, double *const Aarray_[],
+                           int const ldAarray_[], double *const Barray_[], int const ldBarray_[],
+                           double beta, double *const Carray_[], int const ldCarray_[],
+                           int batchCount, kron_stream_t stream);
+int kgemm_tt_batched_async(int mm, int nn, int kk, double alpha, double *const Aarray_[],
+                           int const ldAarray_[], double *const Barray_[], int const ldBarray_[],
+                           double beta, double *const Carray_[], int const ldCarray_[],
+                           int batchCount, kron_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Workspace queries (no reference counterpart): bytes of W the
+ * corresponding call needs; 0 means W may be NULL.
+ * ---------------------------------------------------------------------- */
+size_t kron_batched_workspace_bytes(int d, int n, int batchCount);
+size_t kron_vbatched_workspace_bytes(int d, int const m[], int const n[], int batchCount);
+
+/* ------------------------------------------------------------------------
+ * Precision extensions of the batched layout (no reference counterpart).
+ *   kronmult_batched_f32_async   : FP32 storage, FP32 accumulation.
+ *   kronmult_batched_split_async : FP64 storage; every product is formed
+ *     from hi+lo FP32 parts of A and X (three cross products, error-free
+ *     FP32 products and compensated FP32 sums), and the result is added to
+ *     Y in FP64.
+ * d is 1..6; W as in batched (may be NULL when n^d fits on chip).
+ * ---------------------------------------------------------------------- */
+int kronmult_batched_f32_async(int d, int n, float const A[], float X[], float Y[], float W[],
+                               int batchCount, kron_stream_t stream);
+int kronmult_batched_split_async(int d, int n, double const A[], double X[], double Y[],
+                                 double W[], int batchCount, kron_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Deterministic (bitwise reproducible) accumulation for aliasing outputs
+ * (no reference counterpart).  A segment plan groups the entries by output
+ * pointer once (stable, keeps each group's entry order); an execution with
+ * the plan sums every group in that fixed order on one thread block and
+ * writes each output exactly once -- no atomics.
+ * kron_segments_create reads the device pointer array Yarray_ (batchCount
+ * entries) and synchronises `stream`.
+ * ---------------------------------------------------------------------- */
+typedef struct kron_segments_st *kron_segments_t;
+
+int kron_segments_create(kron_segments_t *plan, double *const Yarray_[], int batchCount,
+                         kron_stream_t stream);
+int kron_segments_destroy(kron_segments_t plan);
+int kron_segments_count(kron_segments_t plan);
+
+int kronmult_xbatched_segmented_async(int d, int n, double const *const Aarray_[], int lda,
+                                      double *Xarray_[], double *Yarray_[], double *Warray_[],
+                                      int batchCount, kron_segments_t plan,
+                                      kron_stream_t stream);
+int kronmult_pbatched_segmented_async(int d, int n, double const Aarray_[], double *Xarray_[],
+                                      double *Yarray_[], double *Warray_[], int batchCount,
+                                      kron_segments_t plan, kron_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Uneven batch (no reference counterpart): every entry has its own d and
+ * rectangular shapes.  shapes (host) holds 13 ints per entry:
+ * {d, m1, n1, m2, n2, ..., m6, n6}.  The plan orders the entries by cost
+ * (largest first) for one persistent launch, picks Alg. 993 forward or
+ * backward per entry by flop count (kronm.hpp:39-89), and sizes the
+ * workspace for the chosen variant.  Execution reads entry k's A_l from
+ * Aarray_[(l-1) + 6*(k-1)] (leading dimension m_l), X from pX_[k], adds
+ * into pY_[k] (outputs may alias).
+ * ---------------------------------------------------------------------- */
+typedef struct kron_vplan_st *kron_vplan_t;
+
+int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const shapes[]);
+int kron_vplan_destroy(kron_vplan_t plan);
+size_t kron_vplan_workspace_bytes(kron_vplan_t plan);
+double kron_vplan_flops(kron_vplan_t plan);
+int kron_vplan_execute_async(kron_vplan_t plan, double const *const Aarray_[], double *pX_[],
+                             double *pY_[], void *W, size_t Wcapacity_bytes,
+                             kron_stream_t stream);
+
+/* kron_flops (kroncommon.hpp:154-185) restated: flops of one entry of the
+ * recursive algorithm. */
+double kron_flops_c(int d, int const m[], int const n[]);
+
+#ifdef __cplusplus
+} /* extern "C" */
+
+/* ------------------------------------------------------------------------
+ * The reference signatures, C++ linkage (mangled names identical to the
+ * reference wrappers', e.g. _Z17kronmult6_batchediPKdPdS1_S1_i).  Each
+ * forwards to its _async twin on stream 0 and records the status.
+ * ---------------------------------------------------------------------- */
+void kronmult1_batched(int n, double const Aarray_[], double Xarray_[], double Yarray_[],
+                       double Warray_[], int batchCount);
+void kronmult2_batched(int n, double const Aarray_[], double Xarray_[], double Yarray_[],
+                       double Warray_[], int batchCount);
+void kronmult3_batched(int n, double const Aarray_[], double Xarray_[], double Yarray_[],
+                       double Warray_[], int batchCount);
+void kronmult4_batched(int n, double const Aarray_[], double Xarray_[], double Yarray_[],
+                       double Warray_[], int batchCount);
+void kronmult5_batched(int n, double const Aarray_[], double Xarray_[], double Yarray_[],
+                       double Warray_[], int batchCount);
+void kronmult6_batched(int n, double const Aarray_[], double Xarray_[], double Yarray_[],
+                       double Warray_[], int batchCount);
+
+void kronmult1_pbatched(int n, double const Aarray_[], double *Xarray_[], double *Yarray_[],
+                        double *Warray_[], int batchCount);
+void kronmult2_pbatched(int n, double const Aarray_[], double *Xarray_[], double *Yarray_[],
+                        double *Warray_[], int batchCount);
+void kronmult3_pbatched(int n, double const Aarray_[], double *Xarray_[], double *Yarray_[],
+                        double *Warray_[], int batchCount);
+void kronmult4_pbatched(int n, double const Aarray_[], double *Xarray_[], double *Yarray_[],
+                        double *Warray_[], int batchCount);
+void kronmult5_pbatched(int n, double const Aarray_[], double *Xarray_[], double *Yarray_[],
+                        double *Warray_[], int batchCount);
+void kronmult6_pbatched(int n, double const Aarray_[], double *Xarray_[], double *Yarray_[],
+                        double *Warray_[], int batchCount);
+
+void kronmult1_xbatched(int n, double const *const Aarray_[], int lda, double *Xarray_[],
+                        double *Yarray_[], double *Warray_[], int batchCount,
+                        int subbatchCount = 0);
+void kronmult2_xbatched(int n, double const *const Aarray_[], int lda, double *Xarray_[],
+                        double *Yarray_[], double *Warray_[], int batchCount,
+                        int subbatchCount = 0);
+void kronmult3_xbatched(int n, double const *const Aarray_[], int lda, double *Xarray_[],
+                        double *Yarray_[], double *Warray_[], int batchCount,
+                        int subbatchCount = 0);
+void kronmult4_xbatched(int n, double const *const Aarray_[], int lda, double *Xarray_[],
+                        double *Yarray_[], double *Warray_[], int batchCount,
+                        int subbatchCount = 0);
+void kronmult5_xbatched(int n, double const *const Aarray_[], int lda, double *Xarray_[],
+                        double *Yarray_[], double *Warray_[], int batchCount,
+                        int subbatchCount = 0);
+void kronmult6_xbatched(int n, double const *const Aarray_[], int lda, double *Xarray_[],
+                        double *Yarray_[], double *Warray_[], int batchCount,
+                        int subbatchCount = 0);
+
+void kronmult1_vbatched(int m1, int n1, double const *const Aarray_[], double *pX_[],
+                        double *pY_[], double *W_, size_t Wcapacity_bytes, int batchCount);
+void kronmult2_vbatched(int m1, int n1, int m2, int n2, double const *const Aarray_[],
+                        double *pX_[], double *pY_[], double *W_, size_t Wcapacity_bytes,
+                        int batchCount);
+void kronmult3_vbatched(int m1, int n1, int m2, int n2, int m3, int n3,
+                        double const *const Aarray_[], double *pX_[], double *pY_[], double *W_,
+                        size_t Wcapacity_bytes, int batchCount);
+void kronmult4_vbatched(int m1, int n1, int m2, int n2, int m3, int n3, int m4, int n4,
+                        double const *const Aarray_[], double *pX_[], double *pY_[], double *W_,
+                        size_t Wcapacity_bytes, int batchCount);
+void kronmult5_vbatched(int m1, int n1, int m2, int n2, int m3, int n3, int m4, int n4, int m5,
+                        int n5, double const *const Aarray_[], double *pX_[], double *pY_[],
+                        double *W_, size_t Wcapacity_bytes, int batchCount);
+void kronmult6_vbatched(int m1, int n1, int m2, int n2, int m3, int n3, int m4, int n4, int m5,
+                        int n5, int m6, int n6, double const *const Aarray_[], double *pX_[],
+                        double *pY_[], double *W_, size_t Wcapacity_bytes, int batchCount);
+
+void kgemm_nn_batched(int mm, int nn, int kk, double alpha, double *const Aarray_[],
+                      int const ldAarray_[], double *const Barray_[], int const ldBarray_[],
+                      double beta, double *const Carray_[], int const ldCarray_[],
+                      int batchCount);
+void kgemm_nt_batched(int mm, int nn, int kk, double alpha, double *const Aarray_[],
+                      int const ldAarray_[], double *const Barray_[], int const ldBarray_[],
+                      double beta, double *const Carray_[], int const ldCarray_[],
+                      int batchCount);
+void kgemm_tt_batched(int mm, int nn, int kk, double alpha, double *const Aarray_[],
+                      int const ldAarray_[], double *const Barray_[], int const ldBarray_[],
+                      double beta, double *const Carray_[], int const ldCarray_[],
+                      int batchCount);
+#endif /* __cplusplus */
+
+#endif /* KRONMULT_B200_H */

@@ -1,0 +1,259 @@
+"""kronmult_b200 -- batched Kronecker matrix-vector products on B200 (sm_100a).
+
+The product is the C-ABI shared library ``kronmult_b200/lib/libkronmult_b200.so``
+(declared in ``include/kronmult.h``).  This module loads it with ctypes and
+offers thin wrappers that take torch CUDA tensors (device memory and streams
+come from PyTorch; all arithmetic runs in the library's CUDA kernels).  There
+is no CPU fallback: if the library is missing or no GPU is present, calls
+raise.
+
+Layouts follow the reference KRONMULT (column major, A_d's index fastest):
+  batched   A (n,n,d,batch) flat, X/Y (n^d, batch) flat
+  pbatched  A as batched, X/Y as tensors of device pointers (int64)
+  xbatched  A as a tensor of d*batch device pointers, common lda
+  vbatched  rectangular shapes, A pointers with ld = m_l
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libkronmult_b200.so")
+INCLUDE_H = os.path.join(os.path.dirname(HERE), "include", "kronmult.h")
+
+_LIB = None
+
+KRON_SUCCESS = 0
+STATUS = {0: "KRON_SUCCESS", 1: "KRON_ERROR_INVALID_VALUE", 2: "KRON_ERROR_WORKSPACE",
+          3: "KRON_ERROR_LAUNCH", 4: "KRON_ERROR_NOT_SUPPORTED", 5: "KRON_ERROR_ALLOC",
+          6: "KRON_ERROR_INTERNAL"}
+
+
+class KronError(RuntimeError):
+    def __init__(self, status, what=""):
+        super().__init__(f"{what}: {STATUS.get(status, status)}")
+        self.status = status
+
+
+def build(verbose: bool = False) -> str:
+    from . import builder as _b
+
+    return _b.build(verbose=verbose)
+
+
+_i, _d, _vp, _sz = C.c_int, C.c_double, C.c_void_p, C.c_size_t
+
+
+def _sig(lib):
+    S = {}
+    for D in range(1, 7):
+        S[f"kronmult{D}_batched_async"] = [_i, _vp, _vp, _vp, _vp, _i, _vp]
+        S[f"kronmult{D}_pbatched_async"] = [_i, _vp, _vp, _vp, _vp, _i, _vp]
+        S[f"kronmult{D}_xbatched_async"] = [_i, _vp, _i, _vp, _vp, _vp, _i, _i, _vp]
+        S[f"kronmult{D}_vbatched_async"] = [_i] * (2 * D) + [_vp, _vp, _vp, _vp, _sz, _i, _vp]
+    for op in ("nn", "nt", "tt"):
+        S[f"kgemm_{op}_batched_async"] = [_i, _i, _i, _d, _vp, _vp, _vp, _vp, _d, _vp, _vp, _i,
+                                          _vp]
+    S["kron_batched_workspace_bytes"] = [_i, _i, _i]
+    S["kron_vbatched_workspace_bytes"] = [_i, _vp, _vp, _i]
+    S["kronmult_batched_f32_async"] = [_i, _i, _vp, _vp, _vp, _vp, _i, _vp]
+    S["kronmult_batched_split_async"] = [_i, _i, _vp, _vp, _vp, _vp, _i, _vp]
+    S["kron_segments_create"] = [_vp, _vp, _i, _vp]
+    S["kron_segments_destroy"] = [_vp]
+    S["kron_segments_count"] = [_vp]
+    S["kronmult_xbatched_segmented_async"] = [_i, _i, _vp, _i, _vp, _vp, _vp, _i, _vp, _vp]
+    S["kronmult_pbatched_segmented_async"] = [_i, _i, _vp, _vp, _vp, _vp, _i, _vp, _vp]
+    S["kron_vplan_create"] = [_vp, _i, _vp]
+    S["kron_vplan_destroy"] = [_vp]
+    S["kron_vplan_workspace_bytes"] = [_vp]
+    S["kron_vplan_flops"] = [_vp]
+    S["kron_vplan_execute_async"] = [_vp, _vp, _vp, _vp, _vp, _sz, _vp]
+    S["kron_flops_c"] = [_i, _vp, _vp]
+    S["kron_status_string"] = [_i]
+    S["kron_get_last_status"] = []
+    S["kron_clear_last_status"] = []
+    S["kron_version"] = []
+    for name, args in S.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = _i
+    lib.kron_batched_workspace_bytes.restype = _sz
+    lib.kron_vbatched_workspace_bytes.restype = _sz
+    lib.kron_vplan_workspace_bytes.restype = _sz
+    lib.kron_vplan_flops.restype = _d
+    lib.kron_flops_c.restype = _d
+    lib.kron_status_string.restype = C.c_char_p
+    lib.kron_version.restype = C.c_char_p
+    return lib
+
+
+def lib():
+    """Load libkronmult_b200.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} missing: run `python -m kronmult_b200.builder`")
+        _LIB = _sig(C.CDLL(LIB_PATH))
+    return _LIB
+
+
+def declared_symbols():
+    """Function names declared in include/kronmult.h (extern "C" and C++)."""
+    import re
+
+    txt = open(INCLUDE_H).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?(?:int|void|size_t|double|char)\s*\*?\s*(\w+)\s*\(",
+                       txt, flags=re.M)
+    return sorted(set(names))
+
+
+# ---------------------------------------------------------------- torch helpers
+def _torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("kronmult_b200 needs a CUDA device")
+    return torch
+
+
+def _ptr(t):
+    return None if t is None else t.data_ptr()
+
+
+def _stream(stream):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def _check(rc, what):
+    if rc != KRON_SUCCESS:
+        raise KronError(rc, what)
+
+
+def kronmult_batched(d, n, A, X, Y, W=None, stream=None):
+    """Y(:,k) += kron(A_1..A_d)(k) X(:,k) -- kronmult{d}_batched."""
+    f = getattr(lib(), f"kronmult{d}_batched_async")
+    batch = Y.numel() // (n ** d) if n else 0
+    _check(f(n, _ptr(A), _ptr(X), _ptr(Y), _ptr(W), batch, _stream(stream)),
+           f"kronmult{d}_batched")
+
+
+def kronmult_pbatched(d, n, A, pX, pY, pW=None, stream=None):
+    f = getattr(lib(), f"kronmult{d}_pbatched_async")
+    _check(f(n, _ptr(A), _ptr(pX), _ptr(pY), _ptr(pW), pX.numel(), _stream(stream)),
+           f"kronmult{d}_pbatched")
+
+
+def kronmult_xbatched(d, n, pA, lda, pX, pY, pW=None, subbatch=0, stream=None):
+    f = getattr(lib(), f"kronmult{d}_xbatched_async")
+    _check(f(n, _ptr(pA), lda, _ptr(pX), _ptr(pY), _ptr(pW), pX.numel(), subbatch,
+             _stream(stream)), f"kronmult{d}_xbatched")
+
+
+def kronmult_vbatched(m, n, pA, pX, pY, W=None, stream=None):
+    d = len(m)
+    f = getattr(lib(), f"kronmult{d}_vbatched_async")
+    mn = []
+    for a, b in zip(m, n):
+        mn += [a, b]
+    wbytes = 0 if W is None else W.numel() * W.element_size()
+    _check(f(*mn, _ptr(pA), _ptr(pX), _ptr(pY), _ptr(W), wbytes, pX.numel(), _stream(stream)),
+           f"kronmult{d}_vbatched")
+
+
+def kgemm_batched(op, mm, nn, kk, alpha, pA, ldA, pB, ldB, beta, pC, ldC, stream=None):
+    f = getattr(lib(), f"kgemm_{op}_batched_async")
+    _check(f(mm, nn, kk, float(alpha), _ptr(pA), _ptr(ldA), _ptr(pB), _ptr(ldB), float(beta),
+             _ptr(pC), _ptr(ldC), pC.numel(), _stream(stream)), f"kgemm_{op}_batched")
+
+
+def kronmult_batched_f32(d, n, A, X, Y, W=None, stream=None):
+    batch = Y.numel() // (n ** d)
+    _check(lib().kronmult_batched_f32_async(d, n, _ptr(A), _ptr(X), _ptr(Y), _ptr(W), batch,
+                                            _stream(stream)), "kronmult_batched_f32")
+
+
+def kronmult_batched_split(d, n, A, X, Y, W=None, stream=None):
+    batch = Y.numel() // (n ** d)
+    _check(lib().kronmult_batched_split_async(d, n, _ptr(A), _ptr(X), _ptr(Y), _ptr(W), batch,
+                                              _stream(stream)), "kronmult_batched_split")
+
+
+class Segments:
+    """Deterministic accumulation plan (groups entries by output pointer)."""
+
+    def __init__(self, pY, stream=None):
+        h = C.c_void_p()
+        _check(lib().kron_segments_create(C.byref(h), _ptr(pY), pY.numel(), _stream(stream)),
+               "kron_segments_create")
+        self.handle = h
+        self.batch = pY.numel()
+
+    @property
+    def count(self):
+        return lib().kron_segments_count(self.handle)
+
+    def close(self):
+        if self.handle:
+            lib().kron_segments_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def kronmult_xbatched_segmented(d, n, pA, lda, pX, pY, seg, pW=None, stream=None):
+    _check(lib().kronmult_xbatched_segmented_async(d, n, _ptr(pA), lda, _ptr(pX), _ptr(pY),
+                                                   _ptr(pW), pX.numel(), seg.handle,
+                                                   _stream(stream)),
+           "kronmult_xbatched_segmented")
+
+
+def kronmult_pbatched_segmented(d, n, A, pX, pY, seg, pW=None, stream=None):
+    _check(lib().kronmult_pbatched_segmented_async(d, n, _ptr(A), _ptr(pX), _ptr(pY), _ptr(pW),
+                                                   pX.numel(), seg.handle, _stream(stream)),
+           "kronmult_pbatched_segmented")
+
+
+class VPlan:
+    """Uneven-batch plan; shapes is a host int array of 13 ints per entry."""
+
+    def __init__(self, shapes):
+        import numpy as np
+
+        arr = np.ascontiguousarray(np.asarray(shapes, dtype=np.int32).reshape(-1, 13))
+        h = C.c_void_p()
+        _check(lib().kron_vplan_create(C.byref(h), arr.shape[0], arr.ctypes.data),
+               "kron_vplan_create")
+        self.handle = h
+        self.batch = arr.shape[0]
+
+    @property
+    def workspace_bytes(self):
+        return lib().kron_vplan_workspace_bytes(self.handle)
+
+    @property
+    def flops(self):
+        return lib().kron_vplan_flops(self.handle)
+
+    def execute(self, pA, pX, pY, W=None, stream=None):
+        wbytes = 0 if W is None else W.numel() * W.element_size()
+        _check(lib().kron_vplan_execute_async(self.handle, _ptr(pA), _ptr(pX), _ptr(pY), _ptr(W),
+                                              wbytes, _stream(stream)), "kron_vplan_execute")
+
+    def close(self):
+        if self.handle:
+            lib().kron_vplan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

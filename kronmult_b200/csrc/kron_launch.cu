@@ -1,0 +1,456 @@
+// Host-side dispatch: picks the kernel family for a problem and launches it.
+//
+//  * square n in 2..8 whose n^d vector (and merge buffer) fits a block's
+//    shared memory            -> kron_sq_kernel<T, d, n>   (compile-time shape)
+//  * any other shape that fits -> kron_gen_kernel<T>        (runtime shape)
+//  * vectors too large for shared memory -> two launches of kron_gen_kernel
+//    through the caller's workspace W: phase 1 applies the trailing modes to
+//    every contiguous block of x (writing W), phase 2 applies the leading
+//    modes to column tiles of W and accumulates into y.
+#include <algorithm>
+#include <cstdio>
+#include <mutex>
+#include <set>
+#include <utility>
+#include <vector>
+
+#include "kron_launch.h"
+#include "kron_sq_table.cuh"
+
+namespace kron {
+
+const DeviceInfo &device_info()
+{
+  static std::mutex mu;
+  static std::vector<DeviceInfo> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  for (auto &d : cache)
+    if (d.device == dev)
+      return d;
+  DeviceInfo info{};
+  info.device = dev;
+  cudaDeviceGetAttribute(&info.sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaDeviceGetAttribute(&info.max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaDeviceGetAttribute(&info.smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  if (info.sms <= 0)
+    info.sms = 148;
+  if (info.max_smem_optin <= 0)
+    info.max_smem_optin = (int)SMEM_OPTIN_MAX;
+  cache.push_back(info);
+  return cache.back();
+}
+
+// cudaFuncSetAttribute once per (kernel, device, size class).
+static int ensure_smem(const void *fn, size_t bytes)
+{
+  static std::mutex mu;
+  static std::set<std::pair<const void *, int>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (done.count({fn, dev}))
+      return KRON_SUCCESS;
+  }
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)device_info().max_smem_optin);
+  if (e != cudaSuccess)
+    return KRON_ERROR_LAUNCH;
+  std::lock_guard<std::mutex> lock(mu);
+  done.insert({fn, dev});
+  (void)bytes;
+  return KRON_SUCCESS;
+}
+
+static int launch_blocks(const void *fn, int nitems_groups, int ng, int block, size_t smem,
+                         void **args, cudaStream_t stream)
+{
+  int rc = ensure_smem(fn, smem);
+  if (rc != KRON_SUCCESS)
+    return rc;
+  const DeviceInfo &di = device_info();
+  int per_sm           = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  long long want = ((long long)nitems_groups + ng - 1) / ng;
+  long long grid = std::min<long long>(want, (long long)di.sms * per_sm);
+  if (grid < 1)
+    grid = 1;
+  cudaError_t e = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(block), args, smem, stream);
+  return e == cudaSuccess ? KRON_SUCCESS : KRON_ERROR_LAUNCH;
+}
+
+static long long prodl(int d, const int *v)
+{
+  long long p = 1;
+  for (int i = 0; i < d; i++)
+    p *= v[i];
+  return p;
+}
+
+double flops_forward(int d, const int *m, const int *n)
+{
+  double size = (double)prodl(d, n), total = 0.0;
+  for (int l = 0; l < d; l++)
+  {
+    double cols = size / n[l];
+    total += 2.0 * m[l] * cols * n[l];
+    size = m[l] * cols;
+  }
+  return total;
+}
+
+double flops_backward(int d, const int *m, const int *n)
+{
+  double size = (double)prodl(d, n), total = 0.0;
+  for (int l = d - 1; l >= 0; l--)
+  {
+    double rows = size / n[l];
+    total += 2.0 * rows * m[l] * n[l];
+    size = rows * m[l];
+  }
+  return total;
+}
+
+// kronm.hpp:83-89: forward only when strictly cheaper.
+bool choose_forward(int d, const int *m, const int *n)
+{
+  return flops_forward(d, m, n) < flops_backward(d, m, n);
+}
+
+// Largest intermediate (elements) along the chosen order, input included.
+long long max_intermediate(int d, const int *m, const int *n, bool forward)
+{
+  int dims[MAXD];
+  for (int l = 0; l < d; l++)
+    dims[l] = n[l];
+  long long best = prodl(d, dims);
+  for (int s = 0; s < d; s++)
+  {
+    int l   = forward ? s : d - 1 - s;
+    dims[l] = m[l];
+    best    = std::max(best, prodl(d, dims));
+  }
+  return best;
+}
+
+static int round_up(long long v, int q) { return (int)((v + q - 1) / q * q); }
+
+static int pick_gs(long long work)
+{
+  if (work >= 2048)
+    return 256;
+  if (work >= 512)
+    return 128;
+  if (work >= 128)
+    return 64;
+  return 32;
+}
+
+// Per-group shared-memory elements of a whole-vector runtime launch.
+static bool gen_whole_view(int d, const int *m, const int *n, bool merge, int esize, GenView &v)
+{
+  v       = GenView{};
+  v.dd    = d;
+  v.mode0 = 0;
+  for (int l = 0; l < d; l++)
+  {
+    v.mm[l] = m[l];
+    v.nn[l] = n[l];
+  }
+  v.forward      = choose_forward(d, m, n) ? 1 : 0;
+  v.subs         = 1;
+  v.C            = 1;
+  v.total_cols   = 0;
+  v.in_row       = 1;
+  v.out_row      = 1;
+  const int q    = 16 / esize;
+  long long mi   = max_intermediate(d, m, n, v.forward != 0);
+  v.max_inter    = round_up(mi, q);
+  v.out_elems    = round_up(prodl(d, m), q);
+  long long asz  = 0;
+  for (int l = 0; l < d; l++)
+    asz += (long long)m[l] * n[l];
+  v.asz          = (int)asz;
+  v.merge        = merge ? 1 : 0;
+  long long ge   = 2LL * v.max_inter + (merge ? v.out_elems : 0) + round_up(asz, q);
+  v.group_elems  = (int)std::min<long long>(ge, 1LL << 30);
+  v.GS           = pick_gs(mi);
+  return ge * esize <= (long long)device_info().max_smem_optin;
+}
+
+template <typename T, int PREC>
+static int launch_gen(Params p, const GenView &v, cudaStream_t stream)
+{
+  const void *fn   = reinterpret_cast<const void *>(&kron_gen_kernel<T, PREC>);
+  size_t gbytes    = (size_t)v.group_elems * sizeof(T);
+  const int maxsm  = device_info().max_smem_optin;
+  int ng           = std::max(1, std::min(256 / v.GS, (int)(maxsm / std::max<size_t>(gbytes, 1))));
+  int block        = ng * v.GS;
+  size_t smem      = (size_t)ng * gbytes;
+  void *args[]     = {&p, const_cast<GenView *>(&v)};
+  long long groups = (long long)p.nitems * v.subs;
+  if (groups <= 0)
+    return KRON_SUCCESS;
+  return launch_blocks(fn, (int)std::min<long long>(groups, 1LL << 30), ng, block, smem, args,
+                       stream);
+}
+
+static int launch_gen_prec(int prec, Params p, const GenView &v, cudaStream_t stream)
+{
+  switch (prec)
+  {
+  case PREC_F64: return launch_gen<double, PREC_F64>(p, v, stream);
+  case PREC_F32: return launch_gen<float, PREC_F32>(p, v, stream);
+  case PREC_SPLIT: return launch_gen<double, PREC_SPLIT>(p, v, stream);
+  default: return KRON_ERROR_NOT_SUPPORTED;
+  }
+}
+
+static SqKernelInfo pick_sq(int prec, int d, int n, bool merge)
+{
+  switch (prec)
+  {
+  case PREC_F64: return sq_kernel_f64(d, n, merge);
+  case PREC_F32: return merge ? SqKernelInfo{nullptr, 0, 0} : sq_kernel_f32(d, n);
+  case PREC_SPLIT: return merge ? SqKernelInfo{nullptr, 0, 0} : sq_kernel_split(d, n);
+  default: return {nullptr, 0, 0};
+  }
+}
+
+static bool is_square(const Params &p)
+{
+  for (int l = 0; l < p.d; l++)
+    if (p.m[l] != p.n[0] || p.n[l] != p.n[0])
+      return false;
+  return true;
+}
+
+// Work-item setup for whole-entry launches.
+static void setup_items(Params &p, const Workspace &ws)
+{
+  // positions [ebase, eend) are set by the caller (0..batch for whole calls)
+  p.ibase = 0;
+  if (p.seg_off)
+  {
+    p.nitems = ws.nseg;
+    p.chunk  = 0;
+    return;
+  }
+  if (p.accum == ACC_ATOMIC)
+  {
+    // short runs of consecutive entries per item so equal outputs merge
+    p.chunk = 8;
+  }
+  else
+    p.chunk = 1;
+  p.nitems = (p.eend - p.ebase + p.chunk - 1) / p.chunk;
+}
+
+size_t large_workspace_elems(int d, const int *m, const int *n)
+{
+  LargePlan lp;
+  if (!plan_large(d, m, n, 8, true, lp))
+    return 0;
+  return (size_t)lp.slot_elems;
+}
+
+bool plan_large(int d, const int *m, const int *n, int esize, bool merge, LargePlan &best)
+{
+  const int maxsm = device_info().max_smem_optin;
+  bool found      = false;
+  for (int q = 1; q < d; q++)
+  {
+    // phase 1: modes [q, d) on contiguous blocks; phase 2: modes [0, q) on column tiles
+    GenView v1;
+    if (!gen_whole_view(d - q, m + q, n + q, false, esize, v1))
+      continue;
+    const long long Nhead = prodl(q, n), Mtail = prodl(d - q, m + q);
+    for (int C : {32, 16, 8, 4, 2, 1})
+    {
+      GenView v2;
+      gen_whole_view(q, m, n, merge, esize, v2);
+      const int qv   = 16 / esize;
+      long long mi   = max_intermediate(q, m, n, v2.forward != 0) * C;
+      v2.max_inter   = round_up(mi, qv);
+      v2.out_elems   = round_up(prodl(q, m) * C, qv);
+      long long ge   = 2LL * v2.max_inter + (merge ? v2.out_elems : 0) + round_up(v2.asz, qv);
+      if (ge * esize > maxsm)
+        continue;
+      v2.group_elems = (int)ge;
+      v2.GS          = pick_gs(mi);
+      // prefer the most balanced split, then the widest tile
+      long long score = std::abs((long long)(v1.max_inter) - (long long)(v2.max_inter / C)) -
+                        (long long)C * 1000;
+      if (!found || score < best.score)
+      {
+        best.q          = q;
+        best.v1         = v1;
+        best.v2         = v2;
+        best.C          = C;
+        best.slot_elems = Nhead * Mtail;
+        best.score      = score;
+        found           = true;
+      }
+      break;
+    }
+  }
+  return found;
+}
+
+template <typename T>
+static int launch_large_t(int prec, Params p, const Workspace &ws, cudaStream_t stream)
+{
+  const bool merge = (p.accum == ACC_ATOMIC || p.accum == ACC_SEGMENTED);
+  LargePlan lp;
+  if (!plan_large(p.d, p.m, p.n, sizeof(T), merge, lp))
+    return KRON_ERROR_NOT_SUPPORTED;
+  const int d = p.d, q = lp.q;
+  const long long Ntail = prodl(d - q, p.n + q), Mtail = prodl(d - q, p.m + q);
+  const long long Nhead = prodl(q, p.n);
+
+  // workspace slots
+  long long nslots = 0;
+  GenView v1 = lp.v1, v2 = lp.v2;
+  v1.ws_ptrs = v2.ws_ptrs = nullptr;
+  v1.ws_ptr_step = v2.ws_ptr_step = 1;
+  if (p.layout == LAYOUT_BATCHED)
+  {
+    if (!ws.W || ws.wstride < lp.slot_elems)
+      return KRON_ERROR_WORKSPACE;
+    nslots     = p.eend - p.ebase;
+    v1.ws_base = v2.ws_base = ws.W;
+    v1.ws_stride = v2.ws_stride = ws.wstride;
+  }
+  else if (ws.pW)
+  {
+    if (ws.pw_elems < lp.slot_elems || ws.npW < 1)
+      return KRON_ERROR_WORKSPACE;
+    nslots     = ws.npW;
+    v1.ws_ptrs = v2.ws_ptrs = ws.pW;
+  }
+  else
+  {
+    nslots = (ws.W ? (long long)(ws.Wbytes / (sizeof(T) * (size_t)lp.slot_elems)) : 0);
+    if (nslots < 1)
+      return KRON_ERROR_WORKSPACE;
+    v1.ws_base = v2.ws_base = ws.W;
+    v1.ws_stride = v2.ws_stride = lp.slot_elems;
+  }
+
+  // phase views
+  v1.mode0       = q;
+  v1.subs        = (int)Nhead;
+  v1.C           = 1;
+  v1.in_sub_off  = Ntail;
+  v1.out_sub_off = Mtail;
+  v1.in_ws       = 0;
+  v1.out_ws      = 1;
+  v1.merge       = 0;
+  v2.mode0       = 0;
+  v2.C           = lp.C;
+  v2.subs        = (int)((Mtail + lp.C - 1) / lp.C);
+  v2.total_cols  = Mtail;
+  v2.in_sub_off  = lp.C;
+  v2.out_sub_off = lp.C;
+  v2.in_row      = Mtail;
+  v2.out_row     = Mtail;
+  v2.in_ws       = 1;
+  v2.out_ws      = 0;
+
+  // chunks of positions that fit the slots (segment-aligned when segmented)
+  int pos = p.ebase, seg = 0;
+  const int pend = p.eend;
+  while (pos < pend)
+  {
+    int end  = (int)std::min<long long>(pend, pos + nslots);
+    int seg1 = seg;
+    if (p.seg_off)
+    {
+      // advance whole segments
+      while (seg1 < ws.nseg && ws.seg_host[seg1 + 1] <= pos + nslots)
+        seg1++;
+      if (seg1 == seg)
+        return KRON_ERROR_WORKSPACE; // one output group needs more slots than provided
+      end = ws.seg_host[seg1];
+    }
+    Params p1  = p;
+    p1.seg_off = nullptr;
+    p1.ebase   = pos;
+    p1.eend    = end;
+    p1.chunk   = 1;
+    p1.nitems  = end - pos;
+    v1.slot0   = pos;
+    int rc     = launch_gen_prec(prec, p1, v1, stream);
+    if (rc != KRON_SUCCESS)
+      return rc;
+    Params p2 = p;
+    v2.slot0  = pos;
+    if (p.seg_off)
+    {
+      p2.ibase  = seg;
+      p2.nitems = seg1 - seg;
+    }
+    else
+    {
+      p2.ebase  = pos;
+      p2.eend   = end;
+      p2.chunk  = (p.accum == ACC_ATOMIC) ? 8 : 1;
+      p2.nitems = (end - pos + p2.chunk - 1) / p2.chunk;
+    }
+    rc = launch_gen_prec(prec, p2, v2, stream);
+    if (rc != KRON_SUCCESS)
+      return rc;
+    pos = end;
+    seg = seg1;
+  }
+  return KRON_SUCCESS;
+}
+
+bool fits_on_chip(int d, const int *m, const int *n, int precision, bool merge)
+{
+  GenView v;
+  return gen_whole_view(d, m, n, merge, precision == PREC_F32 ? 4 : 8, v);
+}
+
+int launch_kron(Params p, int prec, const Workspace &ws, cudaStream_t stream)
+{
+  if (p.batch <= 0 || p.eend <= p.ebase)
+    return KRON_SUCCESS;
+  setup_items(p, ws);
+  if (p.nitems <= 0)
+    return KRON_SUCCESS;
+  const bool merge = (p.accum == ACC_ATOMIC || p.accum == ACC_SEGMENTED);
+  const int esize  = (prec == PREC_F32) ? 4 : 8;
+
+  if (is_square(p) && p.n[0] >= 2 && p.n[0] <= 8)
+  {
+    SqKernelInfo ki = pick_sq(prec, p.d, p.n[0], merge);
+    if (!ki.fn && merge)
+      ki = pick_sq(prec, p.d, p.n[0], false); // atomic without run merging
+    if (ki.fn && ki.group_bytes <= (size_t)device_info().max_smem_optin)
+    {
+      int ng      = std::max(1, std::min(256 / ki.GS,
+                                         (int)(device_info().max_smem_optin / ki.group_bytes)));
+      int block   = ng * ki.GS;
+      size_t smem = (size_t)ng * ki.group_bytes;
+      void *args[] = {&p};
+      return launch_blocks(ki.fn, p.nitems, ng, block, smem, args, stream);
+    }
+  }
+
+  GenView v;
+  if (gen_whole_view(p.d, p.m, p.n, merge, esize, v))
+    return launch_gen_prec(prec, p, v, stream);
+  if (merge && gen_whole_view(p.d, p.m, p.n, false, esize, v))
+    return launch_gen_prec(prec, p, v, stream);
+
+  if (prec == PREC_F32)
+    return launch_large_t<float>(prec, p, ws, stream);
+  return launch_large_t<double>(prec, p, ws, stream);
+}
+
+} // namespace kron

@@ -1,0 +1,24 @@
+// Host-side planning helpers shared by the launcher and the C API.
+#pragma once
+
+#include "kron_kernels.cuh"
+
+namespace kron {
+
+double flops_forward(int d, const int *m, const int *n);
+double flops_backward(int d, const int *m, const int *n);
+bool choose_forward(int d, const int *m, const int *n);
+long long max_intermediate(int d, const int *m, const int *n, bool forward);
+
+// Two-phase plan for vectors that exceed shared memory.
+struct LargePlan
+{
+  int q;                 // phase 1 applies modes [q, d), phase 2 modes [0, q)
+  GenView v1, v2;
+  int C;                 // phase-2 tile columns
+  long long slot_elems;  // workspace elements per entry
+  long long score;
+};
+bool plan_large(int d, const int *m, const int *n, int esize, bool merge, LargePlan &lp);
+
+} // namespace kron
