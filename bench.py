@@ -268,7 +268,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={device_index}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -430,8 +430,9 @@ def run_ours(args, world, rank, local):
                     "peak": round(fp64, 3), "unit": "TFLOP/s",
                     "frac": round(flops / wl.launches_per_step / per_launch_s / 1e12 / fp64, 4),
                     "traffic": traffic,
-                    "peak_source": "FP64 DGEMM 8192^3 (cuBLAS, tensor-core FP64) measured in "
-                                   "this run; MEASURED_PEAKS.json has no FP64 figure",
+                    "peak_source": "FP64 tensor-core (mma.sync f64) throughput measured live "
+                                   "by kron_measure_fp64_peak; MEASURED_PEAKS.json has no "
+                                   "FP64 figure",
                     "hbm_gbs_achieved": round(gbs, 1),
                     "hbm_frac": round(gbs / peaks["hbm_gbs"], 4)}
         else:
@@ -468,23 +469,12 @@ def run_ours(args, world, rank, local):
 
 
 def measure_fp64_peak(torch):
-    """FP64 throughput of cuBLAS DGEMM 8192^3 (best of 5), TFLOP/s."""
-    n = 8192
-    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
-    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
-    torch.matmul(a, b)
-    torch.cuda.synchronize()
-    best = 1e9
-    for _ in range(5):
-        s = torch.cuda.Event(enable_timing=True)
-        e = torch.cuda.Event(enable_timing=True)
-        s.record()
-        torch.matmul(a, b)
-        e.record()
-        e.synchronize()
-        best = min(best, s.elapsed_time(e) / 1e3)
-    del a, b
-    return 2.0 * n ** 3 / best / 1e12
+    """FP64 tensor-core throughput of this GPU (mma.sync f64 chains on every
+    SM, measured live by the library), TFLOP/s."""
+    import kronmult_b200 as kb
+
+    tensor, _core = kb.measure_fp64_peak()
+    return tensor
 
 
 def cpu_baseline(wl, args):
@@ -512,7 +502,7 @@ def cpu_baseline(wl, args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=2)

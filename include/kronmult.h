@@ -253,6 +253,11 @@ int kron_vplan_execute_async(kron_vplan_t plan, double const *const Aarray_[], d
  * recursive algorithm. */
 double kron_flops_c(int d, int const m[], int const n[]);
 
+/* Diagnostics (no reference counterpart): measures the current device's
+ * FP64 throughput in TFLOP/s -- tensor-core (mma.sync f64) and CUDA-core
+ * fma -- for roofline reporting.  Synchronises the device; allocates 2 KB. */
+int kron_measure_fp64_peak(double *tensor_tflops, double *cuda_core_tflops);
+
 #ifdef __cplusplus
 } /* extern "C" */
 

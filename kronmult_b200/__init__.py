@@ -74,6 +74,7 @@ def _sig(lib):
     S["kron_get_last_status"] = []
     S["kron_clear_last_status"] = []
     S["kron_version"] = []
+    S["kron_measure_fp64_peak"] = [_vp, _vp]
     for name, args in S.items():
         f = getattr(lib, name)
         f.argtypes = args
@@ -180,6 +181,13 @@ def kronmult_batched_split(d, n, A, X, Y, W=None, stream=None):
     batch = Y.numel() // (n ** d)
     _check(lib().kronmult_batched_split_async(d, n, _ptr(A), _ptr(X), _ptr(Y), _ptr(W), batch,
                                               _stream(stream)), "kronmult_batched_split")
+
+
+def measure_fp64_peak():
+    """(tensor, cuda_core) FP64 TFLOP/s of the current device."""
+    a, b = C.c_double(), C.c_double()
+    _check(lib().kron_measure_fp64_peak(C.byref(a), C.byref(b)), "kron_measure_fp64_peak")
+    return a.value, b.value
 
 
 class Segments:

@@ -9,6 +9,7 @@
 //    modes to column tiles of W and accumulates into y.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <mutex>
 #include <set>
 #include <utility>
@@ -425,6 +426,9 @@ int launch_kron(Params p, int prec, const Workspace &ws, cudaStream_t stream)
     return KRON_SUCCESS;
   const bool merge = (p.accum == ACC_ATOMIC || p.accum == ACC_SEGMENTED);
   const int esize  = (prec == PREC_F32) ? 4 : 8;
+
+  if (mma8_supported(p, prec) && !std::getenv("KRON_DISABLE_MMA8"))
+    return launch_mma8(p, stream);
 
   if (is_square(p) && p.n[0] >= 2 && p.n[0] <= 8)
   {

@@ -21,4 +21,8 @@ struct LargePlan
 };
 bool plan_large(int d, const int *m, const int *n, int esize, bool merge, LargePlan &lp);
 
+// FP64 tensor-core path for square 8x8 factors, d = 3 (kron_mma8.cu).
+bool mma8_supported(const Params &p, int prec);
+int launch_mma8(Params p, cudaStream_t stream);
+
 } // namespace kron
