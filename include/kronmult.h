@@ -258,6 +258,12 @@ double kron_flops_c(int d, int const m[], int const n[]);
  * fma -- for roofline reporting.  Synchronises the device; allocates 2 KB. */
 int kron_measure_fp64_peak(double *tensor_tflops, double *cuda_core_tflops);
 
+/* Device-side status word of the library's kernels: 0 when every bounded
+ * wait completed, 1 after a kernel gave up waiting on an asynchronous copy
+ * (the affected results are then invalid).  Synchronises with the device;
+ * clear != 0 resets the word.  Returns -1 if it cannot be read. */
+int kron_device_status(int clear);
+
 #ifdef __cplusplus
 } /* extern "C" */
 

@@ -75,6 +75,7 @@ def _sig(lib):
     S["kron_clear_last_status"] = []
     S["kron_version"] = []
     S["kron_measure_fp64_peak"] = [_vp, _vp]
+    S["kron_device_status"] = [_i]
     for name, args in S.items():
         f = getattr(lib, name)
         f.argtypes = args

@@ -19,6 +19,8 @@
 // slice of shared memory, so small vectors are packed several per block.
 #pragma once
 
+#include <type_traits>
+
 #include "kron_internal.cuh"
 
 namespace kron {
@@ -102,63 +104,54 @@ __device__ __forceinline__ void group_copy_in(T *dst, const T *src, int count, i
   }
 }
 
-// y (+)= buf (+ acc) for `count` elements, by the group.
+// y (+)= buf (+ acc) for `count` elements, by the group.  The y loads of a
+// batch of iterations are issued before any store (generic pointers would
+// otherwise serialise every load behind the previous store).
 template <typename T>
 __device__ __forceinline__ void group_flush(int accum, T *y, const T *buf, const T *acc,
                                             bool use_acc, int count, int t, int GS)
 {
   constexpr int V = 16 / sizeof(T);
+  constexpr int B = 4; // vectors in flight per thread
   const bool vec  = (accum != ACC_ATOMIC) && ((reinterpret_cast<uintptr_t>(y) & 15) == 0) &&
                    (count % V == 0);
   if (vec)
   {
+    using VT     = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
     const int nv = count / V;
-    if constexpr (sizeof(T) == 8)
+    VT *yv       = reinterpret_cast<VT *>(y);
+    const VT *bv = reinterpret_cast<const VT *>(buf);
+    const VT *av = reinterpret_cast<const VT *>(acc);
+    for (int i0 = t; i0 < nv; i0 += GS * B)
     {
-      double2 *yv       = reinterpret_cast<double2 *>(y);
-      const double2 *bv = reinterpret_cast<const double2 *>(buf);
-      const double2 *av = reinterpret_cast<const double2 *>(acc);
-      for (int i = t; i < nv; i += GS)
+      VT old[B];
+      if (accum != ACC_STORE)
+#pragma unroll
+        for (int b = 0; b < B; b++)
+          if (i0 + b * GS < nv)
+            old[b] = yv[i0 + b * GS];
+#pragma unroll
+      for (int b = 0; b < B; b++)
       {
-        double2 v = bv[i];
+        const int i = i0 + b * GS;
+        if (i >= nv)
+          continue;
+        VT v = bv[i];
+        T *pv = reinterpret_cast<T *>(&v);
         if (use_acc)
         {
-          double2 a = av[i];
-          v.x += a.x;
-          v.y += a.y;
+          VT a        = av[i];
+          const T *pa = reinterpret_cast<const T *>(&a);
+#pragma unroll
+          for (int u = 0; u < V; u++)
+            pv[u] += pa[u];
         }
         if (accum != ACC_STORE)
         {
-          double2 o = yv[i];
-          v.x += o.x;
-          v.y += o.y;
-        }
-        yv[i] = v;
-      }
-    }
-    else
-    {
-      float4 *yv       = reinterpret_cast<float4 *>(y);
-      const float4 *bv = reinterpret_cast<const float4 *>(buf);
-      const float4 *av = reinterpret_cast<const float4 *>(acc);
-      for (int i = t; i < nv; i += GS)
-      {
-        float4 v = bv[i];
-        if (use_acc)
-        {
-          float4 a = av[i];
-          v.x += a.x;
-          v.y += a.y;
-          v.z += a.z;
-          v.w += a.w;
-        }
-        if (accum != ACC_STORE)
-        {
-          float4 o = yv[i];
-          v.x += o.x;
-          v.y += o.y;
-          v.z += o.z;
-          v.w += o.w;
+          const T *po = reinterpret_cast<const T *>(&old[b]);
+#pragma unroll
+          for (int u = 0; u < V; u++)
+            pv[u] += po[u];
         }
         yv[i] = v;
       }
@@ -166,12 +159,30 @@ __device__ __forceinline__ void group_flush(int accum, T *y, const T *buf, const
   }
   else
   {
-    for (int i = t; i < count; i += GS)
+    for (int i0 = t; i0 < count; i0 += GS * B)
     {
-      T v = buf[i];
-      if (use_acc)
-        v += acc[i];
-      y_update(accum, y, i, v);
+      T old[B];
+      if (accum != ACC_ATOMIC && accum != ACC_STORE)
+#pragma unroll
+        for (int b = 0; b < B; b++)
+          if (i0 + b * GS < count)
+            old[b] = y[i0 + b * GS];
+#pragma unroll
+      for (int b = 0; b < B; b++)
+      {
+        const int i = i0 + b * GS;
+        if (i >= count)
+          continue;
+        T v = buf[i];
+        if (use_acc)
+          v += acc[i];
+        if (accum == ACC_ATOMIC)
+          red_add(y + i, v);
+        else if (accum == ACC_STORE)
+          y[i] = v;
+        else
+          y[i] = old[b] + v;
+      }
     }
   }
 }

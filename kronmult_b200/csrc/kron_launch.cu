@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <map>
 #include <mutex>
 #include <set>
 #include <utility>
@@ -43,39 +44,68 @@ const DeviceInfo &device_info()
   return cache.back();
 }
 
-// cudaFuncSetAttribute once per (kernel, device, size class).
-static int ensure_smem(const void *fn, size_t bytes)
+// Per (kernel, device) launch facts, computed once: the dynamic shared
+// memory attribute is raised to the device maximum and the occupancy for a
+// (block, smem) pair is cached (host-side launch cost matters for the
+// microsecond-scale kernels of small batches).
+struct FnKey
+{
+  const void *fn;
+  int dev, block;
+  size_t smem;
+  bool operator<(const FnKey &o) const
+  {
+    if (fn != o.fn)
+      return fn < o.fn;
+    if (dev != o.dev)
+      return dev < o.dev;
+    if (block != o.block)
+      return block < o.block;
+    return smem < o.smem;
+  }
+};
+
+int cached_occupancy(const void *fn, int block, size_t smem, int *per_sm)
 {
   static std::mutex mu;
-  static std::set<std::pair<const void *, int>> done;
+  static std::map<FnKey, int> occ;
+  static std::set<std::pair<const void *, int>> attr;
   int dev = 0;
   cudaGetDevice(&dev);
+  FnKey key{fn, dev, block, smem};
   {
     std::lock_guard<std::mutex> lock(mu);
-    if (done.count({fn, dev}))
+    auto it = occ.find(key);
+    if (it != occ.end())
+    {
+      *per_sm = it->second;
       return KRON_SUCCESS;
+    }
   }
-  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)device_info().max_smem_optin);
-  if (e != cudaSuccess)
-    return KRON_ERROR_LAUNCH;
+  if (!attr.count({fn, dev}))
+  {
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)device_info().max_smem_optin) != cudaSuccess)
+      return KRON_ERROR_LAUNCH;
+  }
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, block, smem) != cudaSuccess || n < 1)
+    n = 1;
   std::lock_guard<std::mutex> lock(mu);
-  done.insert({fn, dev});
-  (void)bytes;
+  attr.insert({fn, dev});
+  occ[key] = n;
+  *per_sm  = n;
   return KRON_SUCCESS;
 }
 
 static int launch_blocks(const void *fn, int nitems_groups, int ng, int block, size_t smem,
                          void **args, cudaStream_t stream)
 {
-  int rc = ensure_smem(fn, smem);
+  int per_sm = 1;
+  int rc     = cached_occupancy(fn, block, smem, &per_sm);
   if (rc != KRON_SUCCESS)
     return rc;
   const DeviceInfo &di = device_info();
-  int per_sm           = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem) != cudaSuccess ||
-      per_sm < 1)
-    per_sm = 1;
   long long want = ((long long)nitems_groups + ng - 1) / ng;
   long long grid = std::min<long long>(want, (long long)di.sms * per_sm);
   if (grid < 1)
@@ -429,6 +459,12 @@ int launch_kron(Params p, int prec, const Workspace &ws, cudaStream_t stream)
 
   if (mma8_supported(p, prec) && !std::getenv("KRON_DISABLE_MMA8"))
     return launch_mma8(p, stream);
+  if (pipe_supported(p, prec) && !std::getenv("KRON_DISABLE_PIPE"))
+  {
+    int rc = launch_pipe(p, prec, stream);
+    if (rc != KRON_ERROR_NOT_SUPPORTED)
+      return rc;
+  }
 
   if (is_square(p) && p.n[0] >= 2 && p.n[0] <= 8)
   {

@@ -5,6 +5,10 @@
 
 namespace kron {
 
+// Raises the kernel's dynamic shared-memory limit once and caches the
+// resident blocks per SM for (block, smem).
+int cached_occupancy(const void *fn, int block, size_t smem, int *per_sm);
+
 double flops_forward(int d, const int *m, const int *n);
 double flops_backward(int d, const int *m, const int *n);
 bool choose_forward(int d, const int *m, const int *n);
@@ -24,5 +28,10 @@ bool plan_large(int d, const int *m, const int *n, int esize, bool merge, LargeP
 // FP64 tensor-core path for square 8x8 factors, d = 3 (kron_mma8.cu).
 bool mma8_supported(const Params &p, int prec);
 int launch_mma8(Params p, cudaStream_t stream);
+
+// TMA-pipelined register-blocked kernel for square n in {2..5}, 4-64 KB
+// vectors (kron_pipe.cu).
+bool pipe_supported(const Params &p, int prec);
+int launch_pipe(Params p, int prec, cudaStream_t stream);
 
 } // namespace kron

@@ -298,6 +298,51 @@ def test_large_vectors_overlapping_outputs(gpu_lib):
     seg.close()
 
 
+@pytest.mark.parametrize("d,n,layout,offset", [
+    (6, 4, "pbatched", 0), (6, 4, "pbatched", 1), (6, 4, "xbatched", 0), (5, 4, "xbatched", 1),
+    (6, 3, "pbatched", 0), (4, 5, "xbatched", 0), (5, 5, "pbatched", 1), (5, 5, "batched", 0),
+])
+def test_pipelined_layouts(gpu_lib, d, n, layout, offset):
+    """The TMA-pipelined kernel (n in 3..5, 4-64 KB vectors) in every layout;
+    offset=1 shifts every vector by 8 bytes so the bulk-copy alignment
+    fallback runs; outputs alias pairwise in the pointer layouts."""
+    rng = np.random.default_rng(900 + 10 * d + n + offset)
+    L, batch = n ** d, 37
+    A = rng.uniform(-1, 1, n * n * d * batch + offset)
+    X = rng.uniform(-1, 1, L * batch + offset)
+    ny = batch if layout == "batched" else (batch + 1) // 2
+    Y0 = rng.uniform(-1, 1, L * ny + offset)
+    ycol = np.arange(batch) if layout == "batched" else np.arange(batch) // 2
+    Yref = Y0.copy()
+    lda = n + 2 if layout == "xbatched" else n
+    Ax = np.zeros(lda * n * d * batch + offset)
+    for k in range(batch):
+        for l in range(d):
+            blk = A[offset + (k * d + l) * n * n: offset + (k * d + l + 1) * n * n].reshape(n, n)
+            Ax[offset + (k * d + l) * lda * n: offset + (k * d + l + 1) * lda * n] = \
+                np.pad(blk, ((0, 0), (0, lda - n))).reshape(-1)
+    src = Ax if layout == "xbatched" else A
+    ap = [src.ctypes.data + 8 * (offset + (k * d + l) * lda * n) for k in range(batch)
+          for l in range(d)]
+    xp = [X.ctypes.data + 8 * (offset + L * k) for k in range(batch)]
+    yp = [Yref.ctypes.data + 8 * (offset + L * int(j)) for j in ycol]
+    oracle.kronmult_general(d, [n] * d, [n] * d, ap, [lda] * d, xp, yp)
+    dA, dX, dY = dev(src), dev(X), dev(Y0)
+    if layout == "batched":
+        assert offset == 0
+        kb.kronmult_batched(d, n, dA, dX, dY)
+    else:
+        pX = ptrs(dX, [offset + L * k for k in range(batch)])
+        pY = ptrs(dY, [offset + L * int(j) for j in ycol])
+        if layout == "pbatched":
+            kb.kronmult_pbatched(d, n, dA[offset:], pX, pY)
+        else:
+            pA = ptrs(dA, [offset + (k * d + l) * lda * n for k in range(batch) for l in range(d)])
+            kb.kronmult_xbatched(d, n, pA, lda, pX, pY)
+    assert rel_err(host(dY), Yref) <= TOL64
+    assert kb.lib().kron_device_status(1) == 0
+
+
 # ------------------------------------------------------------- precision
 @pytest.mark.parametrize("d,n,batch", [(6, 4, 32), (3, 8, 16), (6, 6, 2), (2, 5, 7)])
 def test_fp32_and_split(gpu_lib, d, n, batch):
