@@ -206,6 +206,21 @@ int kronmult_batched_split_async(int d, int n, double const A[], double X[], dou
                                  double W[], int batchCount, kron_stream_t stream);
 
 /* ------------------------------------------------------------------------
+ * No reference counterpart.  The batched FP64 product for callers that
+ * cannot call cudaMalloc where they apply the operator (a stream capture in
+ * global mode, a memory pool that owns all of HBM, a callback handed only
+ * A, X and Y): it takes no W.  Vectors too large for shared memory use one
+ * 16 MiB file-scope device array instead, which every GPU that loads the
+ * library holds until exit.  n^d above 2,097,152 (16 MiB of doubles) is
+ * rejected with KRON_ERROR_WORKSPACE.  Calls share that array: calls that
+ * overlap on the GPU race; calls ordered on one stream are safe.  The first
+ * call on a device looks the array's address up and should precede any
+ * stream capture.  Allocates nothing.
+ * ---------------------------------------------------------------------- */
+int kronmult_batched_noalloc_async(int d, int n, double const A[], double const X[], double Y[],
+                                   int batchCount, kron_stream_t stream);
+
+/* ------------------------------------------------------------------------
  * Deterministic (bitwise reproducible) accumulation for aliasing outputs
  * (no reference counterpart).  A segment plan groups the entries by output
  * pointer once (stable, keeps each group's entry order); an execution with

@@ -59,6 +59,7 @@ def _sig(lib):
     S["kron_vbatched_workspace_bytes"] = [_i, _vp, _vp, _i]
     S["kronmult_batched_f32_async"] = [_i, _i, _vp, _vp, _vp, _vp, _i, _vp]
     S["kronmult_batched_split_async"] = [_i, _i, _vp, _vp, _vp, _vp, _i, _vp]
+    S["kronmult_batched_noalloc_async"] = [_i, _i, _vp, _vp, _vp, _i, _vp]
     S["kron_segments_create"] = [_vp, _vp, _i, _vp]
     S["kron_segments_destroy"] = [_vp]
     S["kron_segments_count"] = [_vp]
