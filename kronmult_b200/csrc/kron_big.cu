@@ -1,0 +1,489 @@
+// Vectors too large for one block's shared memory (d = 5..6 with n = 6..8:
+// 373 KB .. 2 MB per entry in FP64): one thread-block cluster per entry.
+//
+// The d modes split into a head [0, Q) and a tail [Q, d) with
+// LH = n^Q head rows and LT = n^(d-Q) tail columns, x = X[h][t] (t fastest).
+//   phase 1: every head row h (a contiguous LT block of x) gets the tail
+//            modes; a warp per block (for n = 8 in FP64 the 512-element
+//            FP64 tensor-core routine of kron_mma8_core.cuh), result -> W;
+//   barrier.cluster (hardware, no spinning) -- W is complete;
+//   phase 2: every column tile (LH rows x C columns of W, C contiguous
+//            doubles per row) gets the head modes in shared memory and is
+//            added into y (batched loads before stores, or red.global.add
+//            for aliasing outputs).
+// This is the recursive algorithm's two-level split (kronmultv_recur.hpp:
+// 117-145 applies A_1 on X viewed as (n2..nd) x n1, then recurses), with
+// the intermediate W kept L2-resident: only one entry per cluster is in
+// flight, so the live W is (#clusters x n^d) elements.  The next entry's x
+// and this entry's y are prefetched into L2 while the cluster computes.
+#include <algorithm>
+#include <cstdint>
+#include <cstdlib>
+
+#include "kron_launch.h"
+#include "kron_mma8_core.cuh"
+
+namespace kron {
+
+namespace {
+
+constexpr int BIG_THREADS = 256;
+constexpr int BIG_WARPS   = BIG_THREADS / 32;
+
+__device__ __forceinline__ void cluster_sync_all()
+{
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\t"
+               "barrier.cluster.wait.acquire.aligned;" ::
+                   : "memory");
+}
+
+__device__ __forceinline__ unsigned cluster_rank()
+{
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+__device__ __forceinline__ unsigned cluster_size()
+{
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+
+__device__ __forceinline__ void prefetch_l2(const void *p, long long bytes)
+{
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  const uintptr_t b = (a + 15) & ~uintptr_t(15);
+  const long long n = (bytes - (long long)(b - a)) & ~15LL;
+  if (n >= 16)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b), "r"((unsigned)n)
+                 : "memory");
+}
+
+// Workspace slot for cluster cid working on entry k at position e of the
+// launch range [ebase, eend).
+struct BigWS
+{
+  void *base;
+  long long stride;     // elements between slots (base form)
+  void *const *ptrs;    // pointer form
+  int per_entry;        // 1: a slot per entry; 0: a slot per cluster
+};
+
+template <typename T>
+__device__ __forceinline__ T *big_slot(const BigWS &ws, int k, int e, int ebase, int cid)
+{
+  if (!ws.per_entry)
+    return ws.ptrs ? static_cast<T *>(ws.ptrs[cid])
+                   : static_cast<T *>(ws.base) + (long long)cid * ws.stride;
+  // pointer form: the caller's W pointer of entry k; base form: slot
+  // (e - ebase) of a buffer that covers exactly this launch's range
+  return ws.ptrs ? static_cast<T *>(ws.ptrs[k])
+                 : static_cast<T *>(ws.base) + (long long)(e - ebase) * ws.stride;
+}
+
+template <typename T, int D, int N, int Q, int C>
+struct BigShape
+{
+  static constexpr int LH   = cpow(N, Q);
+  static constexpr int LT   = cpow(N, D - Q);
+  static constexpr int L    = LH * LT;
+  static constexpr int ASZ  = (D * N * N + 15) / 16 * 16;
+  static constexpr bool MMA = (sizeof(T) == 8) && (N == 8) && (D - Q == 3);
+  // phase 1 without tensor cores: rounds of NB head rows share the block's
+  // threads (LT/N fibres per row and mode)
+  static constexpr int FPB  = LT / N;
+  static constexpr int NB   = (BIG_THREADS / FPB) > 0 ? (BIG_THREADS / FPB) : 1;
+  static constexpr int RBUF = ((MMA ? 512 * BIG_WARPS : NB * LT) + 15) / 16 * 16;
+  static constexpr int TBUF = (LH * C + 15) / 16 * 16;
+  static constexpr size_t OFF_A    = 0;
+  static constexpr size_t OFF_R    = OFF_A + (size_t)ASZ * sizeof(T);           // 2 round buffers
+  static constexpr size_t OFF_TILE = OFF_R + 2 * (size_t)RBUF * sizeof(T);      // 2 tile buffers
+  static constexpr size_t SMEM     = OFF_TILE + 2 * (size_t)TBUF * sizeof(T);
+};
+
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src)
+{
+  unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int Nleft>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(Nleft) : "memory"); }
+
+// One mode pass (mode stride S, N-element fibres) over `nblk` consecutive
+// buffers of `blen` elements, fibres spread over the block's threads;
+// A_m (N x N, column major in shared memory) in registers.
+template <typename T, int N, int S, int FPB>
+__device__ __forceinline__ void cta_mode_pass(T *buf, int blen, int nfib, const T *Am, int tid)
+{
+  T a[N][N];
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++)
+      a[i][j] = Am[i + j * N];
+  for (int f = tid; f < nfib; f += BIG_THREADS)
+  {
+    const int bi = f / FPB, ff = f - (f / FPB) * FPB;
+    const int o = ff / S, r = ff - (ff / S) * S;
+    T *b = buf + bi * blen + o * N * S + r;
+    T x[N];
+#pragma unroll
+    for (int j = 0; j < N; j++)
+      x[j] = b[j * S];
+#pragma unroll
+    for (int i = 0; i < N; i++)
+    {
+      T z = T(0);
+#pragma unroll
+      for (int j = 0; j < N; j++)
+        z = fma(a[i][j], x[j], z);
+      b[i * S] = z;
+    }
+  }
+}
+
+// tail modes m = Q..D-1 on the round buffer (compile-time strides)
+template <typename T, int D, int N, int Q, int m>
+__device__ __forceinline__ void round_tail_passes(T *buf, int nrows, const T *As, int tid)
+{
+  if constexpr (m < D)
+  {
+    constexpr int LT  = cpow(N, D - Q);
+    constexpr int S   = cpow(N, D - 1 - m);
+    constexpr int FPB = LT / N;
+    cta_mode_pass<T, N, S, FPB>(buf, LT, nrows * FPB, As + m * N * N, tid);
+    __syncthreads();
+    round_tail_passes<T, D, N, Q, m + 1>(buf, nrows, As, tid);
+  }
+}
+
+// head modes m = 0..Q-1 on a tile (LH rows x C columns, column fastest)
+template <typename T, int N, int Q, int C, int m>
+__device__ __forceinline__ void tile_head_passes(T *tile, const T *As, int tid)
+{
+  if constexpr (m < Q)
+  {
+    constexpr int LH  = cpow(N, Q);
+    constexpr int SR  = cpow(N, Q - 1 - m) * C; // element stride of mode m
+    constexpr int FPB = LH * C / N;
+    cta_mode_pass<T, N, SR, FPB>(tile, 0, FPB, As + m * N * N, tid);
+    __syncthreads();
+    tile_head_passes<T, N, Q, C, m + 1>(tile, As, tid);
+  }
+}
+
+template <typename T, int D, int N, int Q, int C, int MINB>
+__global__ void __launch_bounds__(BIG_THREADS, MINB)
+    kron_big_kernel(const __grid_constant__ Params p, const __grid_constant__ BigWS ws)
+{
+  using S            = BigShape<T, D, N, Q, C>;
+  constexpr int LH   = S::LH;
+  constexpr int LT   = S::LT;
+  constexpr int L    = S::L;
+  extern __shared__ __align__(128) unsigned char smem[];
+  T *As    = reinterpret_cast<T *>(smem + S::OFF_A);
+  T *rbuf0 = reinterpret_cast<T *>(smem + S::OFF_R);
+  T *tbuf0 = reinterpret_cast<T *>(smem + S::OFF_TILE);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  const int cs   = (int)cluster_size();
+  const int rank = (int)cluster_rank();
+  const int cid  = blockIdx.x / cs;
+  const int ncl  = gridDim.x / cs;
+  const long long tot = p.eend - p.ebase;
+  const int eb = p.ebase + (int)(tot * cid / ncl);
+  const int ee = p.ebase + (int)(tot * (cid + 1) / ncl);
+  if (eb >= ee)
+    return; // the whole cluster leaves together
+
+  const int hb = (int)((long long)LH * rank / cs), he = (int)((long long)LH * (rank + 1) / cs);
+  constexpr int NT = (LT + C - 1) / C;
+  const int tb = (int)((long long)NT * rank / cs), te = (int)((long long)NT * (rank + 1) / cs);
+
+  for (int e = eb; e < ee; ++e)
+  {
+    const int k = entry_index(p, e);
+    EntryRef<T> en;
+    entry_fetch<T>(p, k, D, en);
+    T *w = big_slot<T>(ws, k, e, p.ebase, cid);
+
+    if (tid == 0)
+    {
+      const long long share = (long long)L * sizeof(T) / cs;
+      prefetch_l2(reinterpret_cast<const char *>(en.y) + share * rank, share);
+      if (e + 1 < ee)
+      {
+        EntryRef<T> nx;
+        entry_fetch<T>(p, entry_index(p, e + 1), D, nx);
+        prefetch_l2(reinterpret_cast<const char *>(nx.x) + share * rank, share);
+      }
+    }
+    for (int q = tid; q < D * N * N; q += BIG_THREADS)
+    {
+      const int l = q / (N * N), ij = q - l * (N * N);
+      const int j = ij / N, i = ij - j * N;
+      As[q]       = __ldg(en.A[l] + i + (long long)j * en.ld[l]);
+    }
+    __syncthreads();
+
+    // ---------------- phase 1: tail modes on head rows [hb, he)
+    if constexpr (S::MMA)
+    {
+      const int g = lane >> 2, t = lane & 3;
+      double *blk = reinterpret_cast<double *>(rbuf0) + warp * 512;
+      AFrag8 f;
+      load_afrag8(f, reinterpret_cast<const double *>(en.A[Q]), en.ld[Q],
+                  reinterpret_cast<const double *>(en.A[Q + 1]), en.ld[Q + 1],
+                  reinterpret_cast<const double *>(en.A[Q + 2]), en.ld[Q + 2], g, t);
+      const bool al16 = ((reinterpret_cast<uintptr_t>(en.x) & 15) == 0);
+      for (int h = hb + warp; h < he; h += BIG_WARPS)
+      {
+        const double *xb = reinterpret_cast<const double *>(en.x) + (long long)h * LT;
+        double v[8][2], acc[8][2];
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+        {
+          const double *src = xb + q * 64 + g * 8 + 2 * t;
+          if (al16)
+          {
+            double2 u = __ldg(reinterpret_cast<const double2 *>(src));
+            v[q][0]   = u.x;
+            v[q][1]   = u.y;
+          }
+          else
+          {
+            v[q][0] = __ldg(src);
+            v[q][1] = __ldg(src + 1);
+          }
+          acc[q][0] = acc[q][1] = 0.0;
+        }
+        kron8x3_tile(v, acc, f, blk, g, t);
+        double *wb = reinterpret_cast<double *>(w) + (long long)h * LT;
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+#pragma unroll
+          for (int pp = 0; pp < 2; pp++)
+            wb[(2 * t + pp) * 64 + q * 8 + g] = acc[q][pp];
+      }
+    }
+    else
+    {
+      // rounds of NB consecutive head rows, loads double buffered (cp.async)
+      constexpr int NB = S::NB;
+      auto issue_round = [&](int h0, T *buf) {
+        const int nr  = min(NB, he - h0);
+        const T *src = en.x + (long long)h0 * LT;
+        for (int q = tid; q < nr * LT; q += BIG_THREADS)
+          cp_async_elem(buf + q, src + q);
+        cp_commit();
+      };
+      int cur = 0;
+      if (hb < he)
+        issue_round(hb, rbuf0);
+      for (int h0 = hb; h0 < he; h0 += NB)
+      {
+        T *buf = rbuf0 + cur * S::RBUF;
+        if (h0 + NB < he)
+        {
+          issue_round(h0 + NB, rbuf0 + (cur ^ 1) * S::RBUF);
+          cp_wait<1>();
+        }
+        else
+          cp_wait<0>();
+        __syncthreads();
+        const int nr = min(NB, he - h0);
+        round_tail_passes<T, D, N, Q, Q>(buf, nr, As, tid);
+        T *dst = w + (long long)h0 * LT;
+        for (int q = tid; q < nr * LT; q += BIG_THREADS)
+          dst[q] = buf[q];
+        __syncthreads();
+        cur ^= 1;
+      }
+    }
+    __threadfence();
+    __syncthreads();
+    cluster_sync_all(); // W of this entry is complete
+
+    // ---------------- phase 2: head modes on column tiles [tb, te)
+    {
+      auto issue_tile = [&](int tt, T *buf) {
+        const int c0 = tt * C, cc = min(C, LT - c0);
+        for (int q = tid; q < LH * C; q += BIG_THREADS)
+        {
+          const int h = q / C, c = q - (q / C) * C;
+          if (c < cc)
+            cp_async_elem(buf + q, w + (long long)h * LT + c0 + c);
+          else
+            buf[q] = T(0);
+        }
+        cp_commit();
+      };
+      int cur = 0;
+      if (tb < te)
+        issue_tile(tb, tbuf0);
+      for (int tt = tb; tt < te; ++tt)
+      {
+        T *tile = tbuf0 + cur * S::TBUF;
+        if (tt + 1 < te)
+        {
+          issue_tile(tt + 1, tbuf0 + (cur ^ 1) * S::TBUF);
+          cp_wait<1>();
+        }
+        else
+          cp_wait<0>();
+        __syncthreads();
+        tile_head_passes<T, N, Q, C, 0>(tile, As, tid);
+        const int c0 = tt * C, cc = min(C, LT - c0);
+        constexpr int B = 4;
+        for (int q0 = tid; q0 < LH * C; q0 += BIG_THREADS * B)
+        {
+          T old[B];
+          if (p.accum != ACC_ATOMIC)
+#pragma unroll
+            for (int b = 0; b < B; b++)
+            {
+              const int q = q0 + b * BIG_THREADS;
+              const int i = q / C, c = q - (q / C) * C;
+              if (q < LH * C && c < cc)
+                old[b] = en.y[(long long)i * LT + c0 + c];
+            }
+#pragma unroll
+          for (int b = 0; b < B; b++)
+          {
+            const int q = q0 + b * BIG_THREADS;
+            const int i = q / C, c = q - (q / C) * C;
+            if (q < LH * C && c < cc)
+            {
+              T *dst = en.y + (long long)i * LT + c0 + c;
+              if (p.accum == ACC_ATOMIC)
+                red_add(dst, tile[q]);
+              else
+                *dst = old[b] + tile[q];
+            }
+          }
+        }
+        __syncthreads();
+        cur ^= 1;
+      }
+    }
+    cluster_sync_all(); // every block is done with this entry's W
+  }
+}
+
+template <typename T, int D, int N, int Q, int C, int MINB>
+int launch_big_t(Params p, const Workspace &wsp, int prec, cudaStream_t stream)
+{
+  using S        = BigShape<T, D, N, Q, C>;
+  const void *fn = reinterpret_cast<const void *>(&kron_big_kernel<T, D, N, Q, C, MINB>);
+  if (S::SMEM > (size_t)device_info().max_smem_optin)
+    return KRON_ERROR_NOT_SUPPORTED;
+  int dummy = 1;
+  if (cached_occupancy(fn, BIG_THREADS, S::SMEM, &dummy) != KRON_SUCCESS)
+    return KRON_ERROR_LAUNCH;
+
+  // workspace slots: one per entry when the caller's W has them, else one
+  // per cluster
+  BigWS ws{};
+  long long nslots_cluster = 1LL << 30;
+  if (p.layout == LAYOUT_BATCHED)
+  {
+    if (!wsp.W || wsp.wstride < S::L)
+      return KRON_ERROR_WORKSPACE;
+    ws.base      = wsp.W;
+    ws.stride    = wsp.wstride;
+    ws.per_entry = 1;
+  }
+  else if (wsp.pW)
+  {
+    if (wsp.pw_elems < S::L || wsp.npW < 1)
+      return KRON_ERROR_WORKSPACE;
+    ws.ptrs = wsp.pW;
+    if (p.layout == LAYOUT_PBATCHED && wsp.npW >= p.batch)
+      ws.per_entry = 1;
+    else
+      nslots_cluster = wsp.npW;
+  }
+  else
+  {
+    nslots_cluster = wsp.W ? (long long)(wsp.Wbytes / (sizeof(T) * (size_t)S::L)) : 0;
+    if (nslots_cluster < 1)
+      return KRON_ERROR_WORKSPACE;
+    ws.base   = wsp.W;
+    ws.stride = S::L;
+  }
+
+  const long long work = p.eend - p.ebase;
+  int cs               = 2;
+  if (const char *env = std::getenv("KRON_BIG_CLUSTER"))
+    cs = std::max(1, std::min(8, std::atoi(env)));
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id               = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim             = dim3(BIG_THREADS);
+  cfg.dynamicSmemBytes     = S::SMEM;
+  cfg.stream               = stream;
+  cfg.attrs                = attr;
+  cfg.numAttrs             = 1;
+  int ncl                  = 0;
+  cfg.gridDim              = dim3((device_info().sms / cs) * cs);
+  if (cudaOccupancyMaxActiveClusters(&ncl, fn, &cfg) != cudaSuccess || ncl < 1)
+    ncl = std::max(1, device_info().sms / cs);
+  ncl         = (int)std::min<long long>({(long long)ncl, work, nslots_cluster});
+  cfg.gridDim = dim3(ncl * cs);
+  void *args[] = {&p, &ws};
+  return cudaLaunchKernelExC(&cfg, fn, args) == cudaSuccess ? KRON_SUCCESS : KRON_ERROR_LAUNCH;
+}
+
+} // namespace
+
+bool big_supported(const Params &p, int prec)
+{
+  if (prec == PREC_SPLIT || p.accum == ACC_SEGMENTED || p.accum == ACC_STORE)
+    return false;
+  const int n = p.n[0];
+  for (int l = 0; l < p.d; l++)
+    if (p.m[l] != n || p.n[l] != n)
+      return false;
+  if (p.d == 6)
+    return n >= 6 && n <= 8;
+  if (p.d == 5)
+    return n == 8;
+  return false;
+}
+
+int launch_big(Params p, const Workspace &ws, int prec, cudaStream_t stream)
+{
+  if (p.eend <= p.ebase)
+    return KRON_SUCCESS;
+  const int n = p.n[0];
+  // (T, d, n, head modes, tile columns, blocks per SM)
+  if (prec == PREC_F32)
+  {
+    if (p.d == 6 && n == 7)
+      return launch_big_t<float, 6, 7, 3, 32, 2>(p, ws, prec, stream);
+    if (p.d == 6 && n == 8)
+      return launch_big_t<float, 6, 8, 3, 16, 2>(p, ws, prec, stream);
+    return KRON_ERROR_NOT_SUPPORTED;
+  }
+  if (p.d == 6 && n == 6)
+    return launch_big_t<double, 6, 6, 3, 16, 2>(p, ws, prec, stream);
+  if (p.d == 6 && n == 7)
+    return launch_big_t<double, 6, 7, 3, 8, 2>(p, ws, prec, stream);
+  if (p.d == 6 && n == 8)
+    return launch_big_t<double, 6, 8, 3, 16, 1>(p, ws, prec, stream);
+  if (p.d == 5 && n == 8)
+    return launch_big_t<double, 5, 8, 2, 32, 1>(p, ws, prec, stream);
+  return KRON_ERROR_NOT_SUPPORTED;
+}
+
+} // namespace kron

@@ -488,6 +488,12 @@ int launch_kron(Params p, int prec, const Workspace &ws, cudaStream_t stream)
   if (merge && gen_whole_view(p.d, p.m, p.n, false, esize, v))
     return launch_gen_prec(prec, p, v, stream);
 
+  if (big_supported(p, prec) && !std::getenv("KRON_DISABLE_BIG"))
+  {
+    int rc = launch_big(p, ws, prec, stream);
+    if (rc != KRON_ERROR_NOT_SUPPORTED)
+      return rc;
+  }
   if (prec == PREC_F32)
     return launch_large_t<float>(prec, p, ws, stream);
   return launch_large_t<double>(prec, p, ws, stream);

@@ -34,4 +34,8 @@ int launch_mma8(Params p, cudaStream_t stream);
 bool pipe_supported(const Params &p, int prec);
 int launch_pipe(Params p, int prec, cudaStream_t stream);
 
+// Cluster two-phase kernel for vectors beyond shared memory (kron_big.cu).
+bool big_supported(const Params &p, int prec);
+int launch_big(Params p, const Workspace &ws, int prec, cudaStream_t stream);
+
 } // namespace kron

@@ -25,6 +25,7 @@
 #include <cstdint>
 
 #include "kron_launch.h"
+#include "kron_mma8_core.cuh"
 
 namespace kron {
 
@@ -33,22 +34,6 @@ namespace {
 constexpr int WARPS     = 8;        // warps per block
 constexpr int XBUF      = 512;      // doubles per X staging buffer
 constexpr int WARP_SMEM = 2 * XBUF; // doubles per warp (8 KB)
-
-__device__ __forceinline__ void mma884(double &d0, double &d1, double a, double b)
-{
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
-}
-
-__device__ __forceinline__ void mma1688(double &c0, double &c1, double &c2, double &c3, double a0,
-                                        double a1, double a2, double a3, double b0, double b1)
-{
-  asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
-               "{%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
-               : "+d"(c0), "+d"(c1), "+d"(c2), "+d"(c3)
-               : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
-}
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
 {
@@ -89,24 +74,9 @@ __device__ __forceinline__ void stage_x(double *buf, const double *x, int lane)
   cp_async_commit();
 }
 
-struct AFrag
+__device__ __forceinline__ void load_afrag(AFrag8 &f, const EntryRef<double> &en, int g, int t)
 {
-  double a3[2]; // A_3(g, 2t+s), s = 0,1   (A operand of the m8n8k4 steps)
-  double b2[2]; // A_2(g, 2t), A_2(g, 2t+1) (B operand, K rows permuted)
-  double b1[2]; // A_1(g, 2t), A_1(g, 2t+1)
-};
-
-__device__ __forceinline__ void load_afrag(AFrag &f, const EntryRef<double> &en, int g, int t)
-{
-  const long long c0 = (long long)(2 * t) * en.ld[0], c1 = (long long)(2 * t + 1) * en.ld[0];
-  f.b1[0] = __ldg(en.A[0] + g + c0);
-  f.b1[1] = __ldg(en.A[0] + g + c1);
-  const long long d0 = (long long)(2 * t) * en.ld[1], d1 = (long long)(2 * t + 1) * en.ld[1];
-  f.b2[0] = __ldg(en.A[1] + g + d0);
-  f.b2[1] = __ldg(en.A[1] + g + d1);
-  const long long e0 = (long long)(2 * t) * en.ld[2], e1 = (long long)(2 * t + 1) * en.ld[2];
-  f.a3[0] = __ldg(en.A[2] + g + e0);
-  f.a3[1] = __ldg(en.A[2] + g + e1);
+  load_afrag8(f, en.A[0], en.ld[0], en.A[1], en.ld[1], en.A[2], en.ld[2], g, t);
 }
 
 // acc[q][p] holds y(i0 = 2t+p, i1 = q, i2 = g): add it into y with
@@ -178,7 +148,7 @@ __global__ void __launch_bounds__(WARPS * 32) kron_n8d3_mma_kernel(const __grid_
   entry_fetch<double>(p, entry_index(p, e), 3, cur);
   if (e + 1 < ee)
     entry_fetch<double>(p, entry_index(p, e + 1), 3, nxt);
-  AFrag fc, fn;
+  AFrag8 fc, fn;
   load_afrag(fc, cur, g, t);
   int buf = 0;
   stage_x(xbase, cur.x, lane);
@@ -213,69 +183,7 @@ __global__ void __launch_bounds__(WARPS * 32) kron_n8d3_mma_kernel(const __grid_
       v[q][1]   = u.y;
     }
 
-    // ---- mode 3 (contract j2): D(i2, j1) = A_3 * X_q, m8n8k4, K = j2 as {2t, 2t+1}
-    double r[8][2];
-#pragma unroll
-    for (int q = 0; q < 8; q++)
-    {
-      r[q][0] = r[q][1] = 0.0;
-      mma884(r[q][0], r[q][1], fc.a3[0], v[q][0]);
-      mma884(r[q][0], r[q][1], fc.a3[1], v[q][1]);
-    }
-    // r[q][p] = T(j0 = q, i2 = g, j1 = 2t+p)
-
-    // ---- mode 2 (contract j1): rows (tile q, i2 = g), K = j1, B = A_2^T
-#pragma unroll
-    for (int rr = 0; rr < 4; rr++)
-    {
-      double c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;
-      mma1688(c0, c1, c2, c3, r[2 * rr][0], r[2 * rr + 1][0], r[2 * rr][1], r[2 * rr + 1][1],
-              fc.b2[0], fc.b2[1]);
-      v[2 * rr][0]     = c0;
-      v[2 * rr][1]     = c1;
-      v[2 * rr + 1][0] = c2;
-      v[2 * rr + 1][1] = c3;
-    }
-    // v[q][p] = U(j0 = q, i2 = g, i1 = 2t+p)
-
-    // ---- transpose P <-> Q inside each quad: 2x2 blocks (i1 pair a, j0 pair b)
-    // block (a, b) of lane-group g at 32-byte slot g*16 + a*4 + (b ^ a); its two
-    // 16-byte halves swap places for odd g so both sides are conflict free.
-    {
-      __syncwarp(); // every lane has read its X tile from xs
-      const int gpar = g & 1;
-#pragma unroll
-      for (int b = 0; b < 4; b++)
-      {
-        double *blk = xs + 4 * (g * 16 + t * 4 + (b ^ t));
-        // half 0: (i1 = 2t, j0 = 2b, 2b+1); half 1: (i1 = 2t+1, ...)
-        *reinterpret_cast<double2 *>(blk + 2 * gpar) = make_double2(v[2 * b][0], v[2 * b + 1][0]);
-        *reinterpret_cast<double2 *>(blk + 2 * (1 - gpar)) =
-            make_double2(v[2 * b][1], v[2 * b + 1][1]);
-      }
-      __syncwarp();
-#pragma unroll
-      for (int a = 0; a < 4; a++)
-      {
-        const double *blk = xs + 4 * (g * 16 + a * 4 + (t ^ a));
-        double2 h0 = *reinterpret_cast<const double2 *>(blk + 2 * gpar);       // i1 = 2a
-        double2 h1 = *reinterpret_cast<const double2 *>(blk + 2 * (1 - gpar)); // i1 = 2a+1
-        r[2 * a][0]     = h0.x; // (i1 = 2a,   j0 = 2t)
-        r[2 * a][1]     = h0.y; // (i1 = 2a,   j0 = 2t+1)
-        r[2 * a + 1][0] = h1.x;
-        r[2 * a + 1][1] = h1.y;
-      }
-    }
-    // r[q][p] = U(i1 = q, i2 = g, j0 = 2t+p)
-
-    // ---- mode 1 (contract j0), accumulate into the output-group sum
-#pragma unroll
-    for (int rr = 0; rr < 4; rr++)
-      mma1688(acc[2 * rr][0], acc[2 * rr][1], acc[2 * rr + 1][0], acc[2 * rr + 1][1],
-              r[2 * rr][0], r[2 * rr + 1][0], r[2 * rr][1], r[2 * rr + 1][1], fc.b1[0],
-              fc.b1[1]);
-    // acc[q][p] = Y(i0 = 2t+p, i1 = q, i2 = g)
-
+    kron8x3_tile(v, acc, fc, xs, g, t);
     const bool same_next = has_next && (nxt.y == cur.y);
     if (!same_next)
       flush_acc(acc, cur.y, g, t);

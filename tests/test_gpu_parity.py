@@ -343,6 +343,54 @@ def test_pipelined_layouts(gpu_lib, d, n, layout, offset):
     assert kb.lib().kron_device_status(1) == 0
 
 
+@pytest.mark.parametrize("d,n,batch,prec,layout", [
+    (6, 7, 3, "f64", "batched"), (6, 8, 2, "f64", "batched"), (5, 8, 5, "f64", "pbatched"),
+    (6, 8, 3, "f64", "xbatched"), (6, 7, 2, "f32", "batched"), (6, 8, 2, "f32", "batched"),
+    (6, 6, 9, "f64", "pbatched"),
+])
+def test_cluster_two_phase(gpu_lib, d, n, batch, prec, layout):
+    """Vectors beyond shared memory: one thread-block cluster per entry,
+    phase 1 (trailing modes, warp per block; FP64 tensor cores for n = 8),
+    phase 2 (leading modes on column tiles).  Pointer layouts alias
+    outputs pairwise and give fewer W slots than entries for xbatched."""
+    torch = _torch()
+    rng = np.random.default_rng(77 + 10 * d + n + batch)
+    L = n ** d
+    A = rng.standard_normal(n * n * d * batch) / np.sqrt(n)
+    X = rng.uniform(-1, 1, L * batch)
+    ny = batch if layout == "batched" else (batch + 1) // 2
+    Y0 = rng.uniform(-1, 1, L * ny)
+    ycol = np.arange(batch) if layout == "batched" else np.arange(batch) // 2
+    Yref = Y0.copy()
+    ap = [A.ctypes.data + 8 * (k * d + l) * n * n for k in range(batch) for l in range(d)]
+    xp = [X.ctypes.data + 8 * L * k for k in range(batch)]
+    yp = [Yref.ctypes.data + 8 * L * int(j) for j in ycol]
+    oracle.kronmult_general(d, [n] * d, [n] * d, ap, [n] * d, xp, yp)
+    dt = torch.float32 if prec == "f32" else torch.float64
+    dA, dX, dY = dev(A, dt), dev(X, dt), dev(Y0, dt)
+    es = 4 if prec == "f32" else 8
+    if layout == "batched":
+        W = torch.empty(L * batch, dtype=dt, device="cuda")
+        if prec == "f32":
+            kb.kronmult_batched_f32(d, n, dA, dX, dY, W)
+        else:
+            kb.kronmult_batched(d, n, dA, dX, dY, W)
+    else:
+        nw = batch if layout == "pbatched" else 2  # xbatched: 2*subbatch pointers
+        Wb = torch.empty(L * nw, dtype=dt, device="cuda")
+        pW = ptrs(Wb, [L * k for k in range(nw)], es)
+        pX = ptrs(dX, [L * k for k in range(batch)], es)
+        pY = ptrs(dY, [L * int(j) for j in ycol], es)
+        if layout == "pbatched":
+            kb.kronmult_pbatched(d, n, dA, pX, pY, pW)
+        else:
+            pA = ptrs(dA, [(k * d + l) * n * n for k in range(batch) for l in range(d)], es)
+            kb.kronmult_xbatched(d, n, pA, n, pX, pY, pW, subbatch=1)
+    tol = TOL32 if prec == "f32" else TOL64
+    assert rel_err(host(dY).astype(np.float64), Yref) <= tol
+    assert kb.lib().kron_device_status(1) == 0
+
+
 # ------------------------------------------------------------- precision
 @pytest.mark.parametrize("d,n,batch", [(6, 4, 32), (3, 8, 16), (6, 6, 2), (2, 5, 7)])
 def test_fp32_and_split(gpu_lib, d, n, batch):
