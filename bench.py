@@ -221,6 +221,105 @@ class BatchedSquare(Workload):
         return float(self.cs) * 2 * self.d * self.n ** (self.d + 1)
 
 
+class UnevenBatch(Workload):
+    """20000 entries, d ~ U{1..6}, every m_l, n_l ~ U{2,3,4,6,8}: one plan
+    (kron_vplan), persistent launches, replayed as a CUDA graph."""
+
+    def __init__(self, nent=20000, seed=SEED + 4):
+        rng = np.random.default_rng(seed)
+        sizes = np.array([2, 3, 4, 6, 8])
+        self.shapes = np.zeros((nent, 13), dtype=np.int32)
+        a_off, x_off, y_off = [], [], []
+        na = nx = ny = 0
+        self.flop = 0.0
+        import oracle as _o  # flop counts only (host arithmetic)
+        for k in range(nent):
+            d = int(rng.integers(1, 7))
+            m = rng.choice(sizes, size=d)
+            n = rng.choice(sizes, size=d)
+            self.shapes[k, 0] = d
+            self.shapes[k, 1:1 + 2 * d:2] = m
+            self.shapes[k, 2:2 + 2 * d:2] = n
+            for l in range(6):
+                a_off.append(na)
+                if l < d:
+                    na += int(m[l] * n[l])
+            x_off.append(nx)
+            nx += int(np.prod(n))
+            y_off.append(ny)
+            ny += int(np.prod(m))
+            self.flop += min(_o.flops_forward(m, n), _o.flops_backward(m, n))
+        self.A = rng.uniform(-1, 1, na)
+        self.X = rng.uniform(-1, 1, nx)
+        self.ny = ny
+        self.a_off, self.x_off, self.y_off = (np.array(v, dtype=np.int64) for v in
+                                              (a_off, x_off, y_off))
+        self.batch = nent
+        self.name = (f"uneven batch: {nent} entries, d~U(1..6), m,n~U{{2,3,4,6,8}}, "
+                     f"one vplan (persistent launches)")
+
+    def flops(self):
+        return self.flop
+
+    def alg_bytes(self):
+        return 8.0 * (self.X.size + 2 * self.ny + self.A.size)
+
+    def setup(self, torch, kb, mode):
+        dev = torch.device("cuda")
+        self.kb = kb
+        self.plan = kb.VPlan(self.shapes)
+        self.dA = torch.from_numpy(self.A).to(dev)
+        self.dX = torch.from_numpy(self.X).to(dev)
+        self.dY = torch.zeros(self.ny, dtype=torch.float64, device=dev)
+        self.pA = (self.dA.data_ptr() + 8 * torch.from_numpy(self.a_off)).to(dev)
+        self.pX = (self.dX.data_ptr() + 8 * torch.from_numpy(self.x_off)).to(dev)
+        self.pY = (self.dY.data_ptr() + 8 * torch.from_numpy(self.y_off)).to(dev)
+        wb = self.plan.workspace_bytes
+        self.dW = torch.empty(max(1, wb // 8), dtype=torch.float64, device=dev) if wb else None
+        self.h = {k: v.cpu().pin_memory() for k, v in dict(A=self.dA, X=self.dX, Y=self.dY,
+                                                          pA=self.pA, pX=self.pX,
+                                                          pY=self.pY).items()}
+        self.hYout = torch.empty_like(self.h["Y"]).pin_memory()
+        self.h2d_bytes = sum(v.numel() * v.element_size() for v in self.h.values())
+        self.d2h_bytes = self.hYout.numel() * 8
+        self.launches_per_step = 2
+
+    def step(self):
+        self.plan.execute(self.pA, self.pX, self.pY, self.dW)
+
+    def e2e_step(self):
+        for k in ("A", "X", "Y", "pA", "pX", "pY"):
+            getattr(self, "d" + k if k in ("A", "X", "Y") else k).copy_(self.h[k],
+                                                                       non_blocking=True)
+        self.step()
+        self.hYout.copy_(self.dY, non_blocking=True)
+
+    def cpu_setup(self, sample_entries):
+        self.cs = min(self.batch, sample_entries)
+        self.cY = np.zeros(self.ny)
+        A, X, Y = self.A, self.X, self.cY
+        self.c_ap = (A.ctypes.data + 8 * self.a_off[: 6 * self.cs]).astype(np.uint64)
+        self.c_xp = (X.ctypes.data + 8 * self.x_off[: self.cs]).astype(np.uint64)
+        self.c_yp = (Y.ctypes.data + 8 * self.y_off[: self.cs]).astype(np.uint64)
+        return self.cs
+
+    def cpu_step(self, ref):
+        # the reference's kronmult{d}_vbatched, one entry per call, entries over
+        # OpenMP threads (recursive variant: its Alg. 993 workspace sizing is
+        # wrong for rectangular A)
+        ref.kronmult_vbatched_entries(self.shapes[: self.cs], self.c_ap, self.c_xp, self.c_yp)
+
+    def cpu_flops(self):
+        import oracle as _o
+        tot = 0.0
+        for k in range(self.cs):
+            d = int(self.shapes[k, 0])
+            m = self.shapes[k, 1:1 + 2 * d:2]
+            n = self.shapes[k, 2:2 + 2 * d:2]
+            tot += min(_o.flops_forward(m, n), _o.flops_backward(m, n))
+        return tot
+
+
 def make_workload(cfg, precision):
     if cfg == 1:
         return BatchedSquare(6, 4, 512, "f64", "uniform")
@@ -229,6 +328,8 @@ def make_workload(cfg, precision):
     if cfg == 3:
         n = int(os.environ.get("KRON_BENCH_N", "4"))
         return BatchedSquare(6, n, 4096, precision, "normal")
+    if cfg == 4:
+        return UnevenBatch()
     raise SystemExit(f"--config {cfg} not available in this bench")
 
 

@@ -84,8 +84,14 @@ int cached_occupancy(const void *fn, int block, size_t smem, int *per_sm)
   }
   if (!attr.count({fn, dev}))
   {
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)device_info().max_smem_optin) != cudaSuccess)
+    // dynamic + static shared memory may not exceed the opt-in maximum
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess)
+      return KRON_ERROR_LAUNCH;
+    const int dyn_max = device_info().max_smem_optin - (int)fa.sharedSizeBytes;
+    if ((long long)smem > dyn_max ||
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max) !=
+            cudaSuccess)
       return KRON_ERROR_LAUNCH;
   }
   int n = 0;

@@ -1,18 +1,25 @@
 // Uneven-batch plans: every entry has its own d and rectangular shapes
 // (no reference counterpart; the reference's vbatched needs one launch per
-// (d, shape) group, kronmult_vbatched.hpp:17-228).
+// (d, shape) group, kronmult_vbatched.hpp:17-228, nearly one per entry at
+// d >= 3 for random shapes).
 //
-// The plan (built once on the host from the shape table) orders entries by
-// cost, largest first, and groups entries of identical shape so each group
-// runs the compile-time or runtime on-chip kernel; entries too large for
-// shared memory take the two-phase workspace path.  Alg. 993 forward or
-// backward order is chosen per shape by flop count (kronm.hpp:39-89).
-// Executions on a non-default stream are captured once into a CUDA graph
-// and replayed while the operand arrays stay the same.
+// kron_vplan_create (host, once) builds a per-entry descriptor table:
+//   - Alg. 993 order per entry: forward only when strictly cheaper
+//     (kronm.hpp:39-89), and the largest intermediate of that order;
+//   - a class by that size: "warp" (<= 512 elements: one warp per entry,
+//     eight entries per block), "block" (fits the block's shared memory
+//     twice: one block per entry), "huge" (beyond: per-block two-phase
+//     split through the workspace, sizes chosen like the uniform path);
+//   - within each class, entries sorted by flops, largest first.
+// kron_vplan_execute_async then runs two persistent launches (huge; block
+// then warp class) that take entries from device work counters, so the
+// largest entries start first and the small ones fill the tail.  On a
+// non-default stream the counter reset and both launches are captured once
+// into a CUDA graph and replayed while the operand arrays stay the same.
 #include <algorithm>
 #include <cstring>
-#include <map>
 #include <new>
+#include <numeric>
 #include <vector>
 
 #include "kron_launch.h"
@@ -21,48 +28,245 @@ using namespace kron;
 
 namespace {
 
-struct ShapeKey
+constexpr int VP_THREADS  = 256;
+constexpr int VP_WARPS    = VP_THREADS / 32;
+constexpr int WARP_MAX    = 512;   // elements of the largest intermediate, warp class
+constexpr int CLS_WARP    = 0, CLS_BLOCK = 1, CLS_HUGE = 2;
+
+struct VDesc
 {
-  int d;
-  int m[MAXD], n[MAXD];
-  bool operator<(const ShapeKey &o) const
-  {
-    if (d != o.d)
-      return d < o.d;
-    for (int l = 0; l < d; l++)
-    {
-      if (m[l] != o.m[l])
-        return m[l] < o.m[l];
-      if (n[l] != o.n[l])
-        return n[l] < o.n[l];
-    }
-    return false;
-  }
+  int k;                // entry index (operands at pA[6k + l], pX[k], pY[k])
+  unsigned char d, fwd, q, C;  // order; huge: head modes q, tile columns C
+  unsigned char m[6], n[6];
+  int mi;               // largest intermediate (elements) of the chosen order
+  int mi2;              // huge: phase-2 buffer elements (tile rows x C)
+  unsigned char fwd1, fwd2, pad[2]; // huge: order of phase 1 / phase 2
 };
 
-struct Group
+struct VParams
 {
-  ShapeKey key;
-  int begin, end;   // positions in perm
-  double cost;      // flops per entry of the chosen variant
-  bool on_chip;
+  const VDesc *desc;
+  int nhuge, nblock, nwarp;   // descriptors: [huge | block | warp]
+  int *counters;              // 3 work counters (zeroed before every execution)
+  const double *const *pA;
+  const double *const *pX;
+  double *const *pY;
+  double *ws;                 // huge class: per-block slot
   long long slot_elems;
+  int block_elems;            // shared elements per block in block mode
 };
+
+// One entry (or one sub-block view of it) computed by a group of GS threads
+// in the shared buffers b0/b1 (each >= v.max_inter) with factors in As.
+__device__ __forceinline__ void vp_group_entry(const GenView &v, bool strided, const double *x,
+                                               double *out, int accum, double *b0, double *b1,
+                                               double *As, const double *const *A,
+                                               const int *ld, int t, int GS, int g)
+{
+  {
+    int o = 0;
+    for (int q = 0; q < v.dd; q++)
+    {
+      const int l = v.mode0 + q, mq = v.mm[q], nq = v.nn[q];
+      for (int u = t; u < mq * nq; u += GS)
+      {
+        const int j = u / mq, i = u - j * mq;
+        As[o + u]   = __ldg(A[l] + i + (long long)j * ld[l]);
+      }
+      o += mq * nq;
+    }
+  }
+  int rows_in = 1, rows_out = 1;
+  for (int q = 0; q < v.dd; q++)
+  {
+    rows_in *= v.nn[q];
+    rows_out *= v.mm[q];
+  }
+  if (!strided)
+    group_copy_in(b0, x, rows_in, t, GS);
+  else
+    for (int q = t; q < rows_in * v.C; q += GS)
+    {
+      const int h = q / v.C, c = q - h * v.C;
+      b0[q]       = (c < v.total_cols) ? __ldg(x + h * v.in_row + c) : 0.0;
+    }
+  group_sync(g, GS);
+  double *cur = b0, *nxt = b1;
+  gen_apply_modes<double, PREC_F64>(v, cur, nxt, As, v.C, t, GS, g);
+  if (!strided)
+    group_flush(accum, out, cur, cur, false, rows_out, t, GS);
+  else
+    for (int q = t; q < rows_out * v.C; q += GS)
+    {
+      const int i = q / v.C, c = q - i * v.C;
+      if (c < v.total_cols)
+        y_update(accum, out + i * v.out_row, c, cur[q]);
+    }
+  group_sync(g, GS);
+}
+
+__device__ __forceinline__ void vp_view(GenView &v, const VDesc &e, int mode0, int dd)
+{
+  v.dd    = dd;
+  v.mode0 = mode0;
+  for (int q = 0; q < dd; q++)
+  {
+    v.mm[q] = e.m[mode0 + q];
+    v.nn[q] = e.n[mode0 + q];
+  }
+  v.forward = e.fwd;
+  v.C       = 1;
+  v.in_row = v.out_row = 1;
+  v.total_cols         = 1;
+}
+
+__device__ __forceinline__ void vp_operands(const VParams &vp, const VDesc &e, const double *A[6],
+                                            int ld[6], const double *&x, double *&y)
+{
+  for (int l = 0; l < 6; l++)
+  {
+    A[l]  = l < e.d ? vp.pA[6LL * e.k + l] : nullptr;
+    ld[l] = l < e.d ? e.m[l] : 1;
+  }
+  x = vp.pX[e.k];
+  y = vp.pY[e.k];
+}
+
+// block class, then warp class, from two work counters
+__global__ void __launch_bounds__(VP_THREADS, 1) kron_vplan_kernel(const __grid_constant__ VParams vp)
+{
+  extern __shared__ __align__(16) double smem[];
+  __shared__ int s_idx;
+  const int tid = threadIdx.x;
+
+  // ---- block class: the whole block per entry
+  const VDesc *blk = vp.desc + vp.nhuge;
+  while (true)
+  {
+    if (tid == 0)
+      s_idx = atomicAdd(&vp.counters[1], 1);
+    __syncthreads();
+    const int idx = s_idx;
+    __syncthreads();
+    if (idx >= vp.nblock)
+      break;
+    const VDesc e = blk[idx];
+    GenView v;
+    vp_view(v, e, 0, e.d);
+    const double *A[6];
+    int ld[6];
+    const double *x;
+    double *y;
+    vp_operands(vp, e, A, ld, x, y);
+    const int mi = (e.mi + 1) & ~1;
+    vp_group_entry(v, false, x, y, ACC_ATOMIC, smem, smem + mi, smem + 2 * mi, A, ld, tid,
+                   VP_THREADS, 0);
+  }
+
+  // ---- warp class: one warp per entry
+  const int warp = tid >> 5, lane = tid & 31;
+  const int slice = vp.block_elems / VP_WARPS;
+  double *b0      = smem + warp * slice;
+  const VDesc *wd = vp.desc + vp.nhuge + vp.nblock;
+  while (true)
+  {
+    int idx = 0;
+    if (lane == 0)
+      idx = atomicAdd(&vp.counters[2], 1);
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+    if (idx >= vp.nwarp)
+      break;
+    const VDesc e = wd[idx];
+    GenView v;
+    vp_view(v, e, 0, e.d);
+    const double *A[6];
+    int ld[6];
+    const double *x;
+    double *y;
+    vp_operands(vp, e, A, ld, x, y);
+    vp_group_entry(v, false, x, y, ACC_ATOMIC, b0, b0 + WARP_MAX, b0 + 2 * WARP_MAX, A, ld, lane,
+                   32, warp);
+  }
+}
+
+// huge class: per block, phase 1 (tail modes on each head block -> slot),
+// phase 2 (head modes on column tiles of the slot -> y)
+__global__ void __launch_bounds__(VP_THREADS, 1)
+    kron_vplan_huge_kernel(const __grid_constant__ VParams vp)
+{
+  extern __shared__ __align__(16) double smem[];
+  __shared__ int s_idx;
+  const int tid = threadIdx.x;
+  double *slot  = vp.ws + (long long)blockIdx.x * vp.slot_elems;
+  while (true)
+  {
+    if (tid == 0)
+      s_idx = atomicAdd(&vp.counters[0], 1);
+    __syncthreads();
+    const int idx = s_idx;
+    __syncthreads();
+    if (idx >= vp.nhuge)
+      break;
+    const VDesc e = vp.desc[idx];
+    const int d = e.d, q = e.q, C = e.C;
+    const double *A[6];
+    int ld[6];
+    const double *x;
+    double *y;
+    vp_operands(vp, e, A, ld, x, y);
+    int Nhead = 1, Ntail = 1, Mtail = 1;
+    for (int l = 0; l < q; l++)
+      Nhead *= e.n[l];
+    for (int l = q; l < d; l++)
+    {
+      Ntail *= e.n[l];
+      Mtail *= e.m[l];
+    }
+    // phase 1 (order and buffer size from the plan)
+    GenView v1;
+    vp_view(v1, e, q, d - q);
+    v1.forward    = e.fwd1;
+    const int mi1 = e.mi;
+    for (int h = 0; h < Nhead; h++)
+      vp_group_entry(v1, false, x + (long long)h * Ntail, slot + (long long)h * Mtail, ACC_STORE,
+                     smem, smem + mi1, smem + 2 * mi1, A, ld, tid, VP_THREADS, 0);
+    __threadfence_block();
+    __syncthreads();
+    // phase 2
+    GenView v2;
+    vp_view(v2, e, 0, q);
+    v2.forward    = e.fwd2;
+    v2.C          = C;
+    v2.in_row = v2.out_row = Mtail;
+    const int mi2 = e.mi2;
+    for (int c0 = 0; c0 < Mtail; c0 += C)
+    {
+      v2.total_cols = min(C, Mtail - c0);
+      vp_group_entry(v2, true, slot + c0, y + c0, ACC_ATOMIC, smem, smem + mi2, smem + 2 * mi2, A,
+                     ld, tid, VP_THREADS, 0);
+    }
+    __syncthreads();
+  }
+}
 
 } // namespace
 
 struct kron_vplan_st
 {
   int batch;
-  std::vector<Group> groups;
-  int *d_perm;
+  int nhuge, nblock, nwarp;
+  VDesc *d_desc;
+  int *d_counters;
   double flops;
+  long long slot_elems;
+  int huge_grid;
   size_t ws_bytes;
+  size_t smem_main, smem_huge;
+  int block_elems;
   // graph cache
   cudaGraphExec_t exec;
   const void *gA, *gX, *gY, *gW;
   size_t gWcap;
-  cudaStream_t gstream;
 };
 
 extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const shapes[])
@@ -70,85 +274,115 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
   if (!plan || batchCount < 0 || (batchCount > 0 && !shapes))
     return KRON_ERROR_INVALID_VALUE;
   *plan = nullptr;
-  std::map<ShapeKey, std::vector<int>> by_shape;
+  const DeviceInfo &di = device_info();
+  const int maxsm      = di.max_smem_optin;
+  // block class: two buffers + factors within the block's shared memory
+  const int block_elems = (maxsm - 4096) / 8;
+  std::vector<VDesc> cls[3];
+  std::vector<double> cost[3];
+  double total_flops   = 0.0;
+  long long max_slot   = 0;
+  size_t smem_huge     = 0;
   for (int k = 0; k < batchCount; k++)
   {
     const int *s = shapes + 13LL * k;
-    ShapeKey key;
-    std::memset(&key, 0, sizeof(key));
-    key.d = s[0];
-    if (key.d < 1 || key.d > MAXD)
+    VDesc e;
+    std::memset(&e, 0, sizeof(e));
+    e.k     = k;
+    const int d = s[0];
+    if (d < 1 || d > MAXD)
       return KRON_ERROR_INVALID_VALUE;
-    for (int l = 0; l < key.d; l++)
+    int m[MAXD], n[MAXD];
+    for (int l = 0; l < d; l++)
     {
-      key.m[l] = s[1 + 2 * l];
-      key.n[l] = s[2 + 2 * l];
-      if (key.m[l] < 1 || key.n[l] < 1)
+      m[l] = s[1 + 2 * l];
+      n[l] = s[2 + 2 * l];
+      if (m[l] < 1 || n[l] < 1 || m[l] > 255 || n[l] > 255)
         return KRON_ERROR_INVALID_VALUE;
+      e.m[l] = (unsigned char)m[l];
+      e.n[l] = (unsigned char)n[l];
     }
-    by_shape[key].push_back(k);
+    e.d              = (unsigned char)d;
+    const bool fwd   = choose_forward(d, m, n);
+    e.fwd            = fwd ? 1 : 0;
+    const long long mi = max_intermediate(d, m, n, fwd);
+    const double fl  = std::min(flops_forward(d, m, n), flops_backward(d, m, n));
+    total_flops += fl;
+    long long asz = 0;
+    for (int l = 0; l < d; l++)
+      asz += (long long)m[l] * n[l];
+    const long long mi2r = (mi + 1) & ~1LL;
+    int c;
+    if (mi <= WARP_MAX && 2 * WARP_MAX + asz <= block_elems / VP_WARPS)
+      c = CLS_WARP;
+    else if (2 * mi2r + asz <= block_elems)
+      c = CLS_BLOCK;
+    else
+    {
+      c = CLS_HUGE;
+      LargePlan lp;
+      if (!plan_large(d, m, n, 8, false, lp) || lp.C > 255)
+        return KRON_ERROR_NOT_SUPPORTED;
+      e.q    = (unsigned char)lp.q;
+      e.C    = (unsigned char)lp.C;
+      e.fwd1 = (unsigned char)lp.v1.forward;
+      e.fwd2 = (unsigned char)lp.v2.forward;
+      e.mi2  = lp.v2.max_inter; // rows x C, rounded
+      max_slot = std::max(max_slot, lp.slot_elems);
+      smem_huge = std::max(smem_huge, (size_t)std::max(lp.v1.group_elems, lp.v2.group_elems) * 8);
+    }
+    e.mi = (c == CLS_HUGE) ? 0 : (int)mi;
+    if (c == CLS_HUGE)
+    {
+      LargePlan lp;
+      plan_large(d, m, n, 8, false, lp);
+      e.mi = lp.v1.max_inter; // phase-1 buffer elements, rounded
+    }
+    cls[c].push_back(e);
+    cost[c].push_back(fl);
   }
   kron_vplan_st *pl = new (std::nothrow) kron_vplan_st();
   if (!pl)
     return KRON_ERROR_ALLOC;
-  pl->batch  = batchCount;
-  pl->d_perm = nullptr;
-  pl->flops  = 0.0;
-  pl->ws_bytes = 0;
-  pl->exec   = nullptr;
-  std::vector<Group> groups;
-  for (auto &kv : by_shape)
+  std::vector<VDesc> all;
+  all.reserve(batchCount);
+  for (int c : {CLS_HUGE, CLS_BLOCK, CLS_WARP})
   {
-    Group g;
-    g.key = kv.first;
-    const ShapeKey &k = kv.first;
-    g.cost = std::min(flops_forward(k.d, k.m, k.n), flops_backward(k.d, k.m, k.n));
-    g.on_chip = fits_on_chip(k.d, k.m, k.n, PREC_F64, true) ||
-                fits_on_chip(k.d, k.m, k.n, PREC_F64, false);
-    g.slot_elems = g.on_chip ? 0 : (long long)large_workspace_elems(k.d, k.m, k.n);
-    if (!g.on_chip && g.slot_elems <= 0)
-    {
-      delete pl;
-      return KRON_ERROR_NOT_SUPPORTED;
-    }
-    g.begin = 0;
-    g.end   = (int)kv.second.size();
-    groups.push_back(g);
-    pl->flops += g.cost * kv.second.size();
+    std::vector<int> order(cls[c].size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return cost[c][a] > cost[c][b]; });
+    for (int i : order)
+      all.push_back(cls[c][i]);
   }
-  // largest per-entry cost first
-  std::vector<int> order(groups.size());
-  for (size_t i = 0; i < order.size(); i++)
-    order[i] = (int)i;
-  std::stable_sort(order.begin(), order.end(),
-                   [&](int a, int b) { return groups[a].cost > groups[b].cost; });
-  std::vector<int> perm;
-  perm.reserve(batchCount);
-  for (int gi : order)
+  pl->batch       = batchCount;
+  pl->nhuge       = (int)cls[CLS_HUGE].size();
+  pl->nblock      = (int)cls[CLS_BLOCK].size();
+  pl->nwarp       = (int)cls[CLS_WARP].size();
+  pl->flops       = total_flops;
+  pl->slot_elems  = max_slot;
+  pl->block_elems = block_elems;
+  pl->smem_main   = (size_t)block_elems * 8;
+  pl->smem_huge   = std::max<size_t>(smem_huge, 16);
+  pl->huge_grid   = pl->nhuge ? std::min(pl->nhuge, di.sms) : 0;
+  pl->ws_bytes    = (size_t)pl->huge_grid * (size_t)max_slot * 8;
+  pl->exec        = nullptr;
+  pl->d_desc      = nullptr;
+  pl->d_counters  = nullptr;
+  if (cudaMalloc(&pl->d_counters, 4 * sizeof(int)) != cudaSuccess ||
+      (batchCount > 0 && cudaMalloc(&pl->d_desc, sizeof(VDesc) * batchCount) != cudaSuccess))
   {
-    Group g   = groups[gi];
-    auto &ids = by_shape[g.key];
-    g.begin   = (int)perm.size();
-    perm.insert(perm.end(), ids.begin(), ids.end());
-    g.end = (int)perm.size();
-    if (!g.on_chip)
-      pl->ws_bytes = std::max(pl->ws_bytes, (size_t)g.slot_elems * (g.end - g.begin) * 8);
-    pl->groups.push_back(g);
+    cudaFree(pl->d_counters);
+    delete pl;
+    return KRON_ERROR_ALLOC;
   }
-  if (batchCount > 0)
+  if (batchCount > 0 && cudaMemcpy(pl->d_desc, all.data(), sizeof(VDesc) * batchCount,
+                                   cudaMemcpyHostToDevice) != cudaSuccess)
   {
-    if (cudaMalloc(&pl->d_perm, sizeof(int) * batchCount) != cudaSuccess)
-    {
-      delete pl;
-      return KRON_ERROR_ALLOC;
-    }
-    if (cudaMemcpy(pl->d_perm, perm.data(), sizeof(int) * batchCount, cudaMemcpyHostToDevice) !=
-        cudaSuccess)
-    {
-      cudaFree(pl->d_perm);
-      delete pl;
-      return KRON_ERROR_LAUNCH;
-    }
+    cudaFree(pl->d_desc);
+    cudaFree(pl->d_counters);
+    delete pl;
+    return KRON_ERROR_LAUNCH;
   }
   *plan = pl;
   return KRON_SUCCESS;
@@ -160,7 +394,8 @@ extern "C" int kron_vplan_destroy(kron_vplan_t plan)
     return KRON_SUCCESS;
   if (plan->exec)
     cudaGraphExecDestroy(plan->exec);
-  cudaFree(plan->d_perm);
+  cudaFree(plan->d_desc);
+  cudaFree(plan->d_counters);
   delete plan;
   return KRON_SUCCESS;
 }
@@ -169,34 +404,44 @@ extern "C" size_t kron_vplan_workspace_bytes(kron_vplan_t plan) { return plan ? 
 extern "C" double kron_vplan_flops(kron_vplan_t plan) { return plan ? plan->flops : 0.0; }
 
 static int vplan_launch_all(kron_vplan_t pl, double const *const *A, double **X, double **Y,
-                            void *W, size_t Wcap, cudaStream_t s)
+                            void *W, cudaStream_t s)
 {
-  for (const Group &g : pl->groups)
+  if (cudaMemsetAsync(pl->d_counters, 0, 4 * sizeof(int), s) != cudaSuccess)
+    return KRON_ERROR_LAUNCH;
+  VParams vp;
+  std::memset(&vp, 0, sizeof(vp));
+  vp.desc        = pl->d_desc;
+  vp.nhuge       = pl->nhuge;
+  vp.nblock      = pl->nblock;
+  vp.nwarp       = pl->nwarp;
+  vp.counters    = pl->d_counters;
+  vp.pA          = A;
+  vp.pX          = X;
+  vp.pY          = Y;
+  vp.ws          = static_cast<double *>(W);
+  vp.slot_elems  = pl->slot_elems;
+  vp.block_elems = pl->block_elems;
+  void *args[]   = {&vp};
+  const int sms  = device_info().sms;
+  if (pl->nhuge > 0)
   {
-    Params p;
-    std::memset(&p, 0, sizeof(p));
-    p.layout = LAYOUT_VBATCHED;
-    p.accum  = ACC_ATOMIC;
-    p.d      = g.key.d;
-    for (int l = 0; l < MAXD; l++)
-    {
-      p.m[l] = l < p.d ? g.key.m[l] : 1;
-      p.n[l] = l < p.d ? g.key.n[l] : 1;
-    }
-    p.apk   = MAXD;
-    p.batch = pl->batch;
-    p.pA    = reinterpret_cast<const void *const *>(A);
-    p.pX    = reinterpret_cast<const void *const *>(X);
-    p.pY    = reinterpret_cast<void *const *>(Y);
-    p.perm  = pl->d_perm;
-    p.ebase = g.begin;
-    p.eend  = g.end;
-    Workspace ws{};
-    ws.W      = W;
-    ws.Wbytes = W ? Wcap : 0;
-    int rc    = launch_kron(p, PREC_F64, ws, s);
-    if (rc != KRON_SUCCESS)
-      return rc;
+    const void *fh = reinterpret_cast<const void *>(&kron_vplan_huge_kernel);
+    int occ        = 1;
+    if (cached_occupancy(fh, VP_THREADS, pl->smem_huge, &occ) != KRON_SUCCESS)
+      return KRON_ERROR_LAUNCH;
+    if (cudaLaunchKernel(fh, dim3(pl->huge_grid), dim3(VP_THREADS), args, pl->smem_huge, s) !=
+        cudaSuccess)
+      return KRON_ERROR_LAUNCH;
+  }
+  if (pl->nblock + pl->nwarp > 0)
+  {
+    const void *fm = reinterpret_cast<const void *>(&kron_vplan_kernel);
+    int occ        = 1;
+    if (cached_occupancy(fm, VP_THREADS, pl->smem_main, &occ) != KRON_SUCCESS)
+      return KRON_ERROR_LAUNCH;
+    const int grid = std::max(1, std::min(sms * occ, pl->nblock + (pl->nwarp + VP_WARPS - 1) / VP_WARPS));
+    if (cudaLaunchKernel(fm, dim3(grid), dim3(VP_THREADS), args, pl->smem_main, s) != cudaSuccess)
+      return KRON_ERROR_LAUNCH;
   }
   return KRON_SUCCESS;
 }
@@ -212,7 +457,7 @@ extern "C" int kron_vplan_execute_async(kron_vplan_t plan, double const *const A
   if (!Aarray_ || !pX_ || !pY_)
     return KRON_ERROR_INVALID_VALUE;
   cudaStream_t s = (cudaStream_t)stream;
-  if (plan->ws_bytes > 0 && (!W || Wcapacity_bytes == 0))
+  if (plan->ws_bytes > 0 && (!W || Wcapacity_bytes < plan->ws_bytes))
     return KRON_ERROR_WORKSPACE;
 
   // Graphs only on explicit streams that are not already capturing.
@@ -221,7 +466,7 @@ extern "C" int kron_vplan_execute_async(kron_vplan_t plan, double const *const A
                    cs == cudaStreamCaptureStatusNone;
   if (!use_graph)
   {
-    int rc = vplan_launch_all(plan, Aarray_, pX_, pY_, W, Wcapacity_bytes, s);
+    int rc = vplan_launch_all(plan, Aarray_, pX_, pY_, W, s);
     if (rc != KRON_SUCCESS)
       return rc;
     return cudaGetLastError() == cudaSuccess ? KRON_SUCCESS : KRON_ERROR_LAUNCH;
@@ -235,10 +480,14 @@ extern "C" int kron_vplan_execute_async(kron_vplan_t plan, double const *const A
       cudaGraphExecDestroy(plan->exec);
       plan->exec = nullptr;
     }
+    // kernel attributes are set outside the capture
+    int rc = vplan_launch_all(plan, Aarray_, pX_, pY_, W, s);
+    if (rc != KRON_SUCCESS)
+      return rc;
     cudaGraph_t graph = nullptr;
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
       return KRON_ERROR_LAUNCH;
-    int rc = vplan_launch_all(plan, Aarray_, pX_, pY_, W, Wcapacity_bytes, s);
+    rc             = vplan_launch_all(plan, Aarray_, pX_, pY_, W, s);
     cudaError_t ce = cudaStreamEndCapture(s, &graph);
     if (rc != KRON_SUCCESS)
     {
@@ -259,6 +508,7 @@ extern "C" int kron_vplan_execute_async(kron_vplan_t plan, double const *const A
     plan->gY    = pY_;
     plan->gW    = W;
     plan->gWcap = Wcapacity_bytes;
+    return KRON_SUCCESS; // this execution ran directly above
   }
   return cudaGraphLaunch(plan->exec, s) == cudaSuccess ? KRON_SUCCESS : KRON_ERROR_LAUNCH;
 }

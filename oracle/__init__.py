@@ -186,6 +186,7 @@ class Reference:
                                               C.c_int]
         lib.ref_kgemm_batched.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, _vp,
                                           _ip, _vp, _ip, C.c_double, _vp, _ip, C.c_int]
+        lib.ref_kronmult_vbatched_entries.argtypes = [C.c_int, _ip, _vp, _vp, _vp, C.c_size_t]
         lib.ref_kron_flops.argtypes = [C.c_int, _ip, _ip]
         lib.ref_kron_flops.restype = C.c_double
         lib.ref_uses_alg993.restype = C.c_int
@@ -236,6 +237,14 @@ class Reference:
         py, pyp = _ptrs(y_ptrs)
         rc = self.lib.ref_kronmult_vbatched(d, mp, np_, pap, pxp, pyp, _d(W), W.nbytes,
                                             len(x_ptrs))
+        assert rc == 0
+
+    def kronmult_vbatched_entries(self, shapes, a_ptrs, x_ptrs, y_ptrs, wbytes=1 << 24):
+        sh, shp = _i(np.asarray(shapes).reshape(-1))
+        pa, pap = _ptrs(a_ptrs)
+        px, pxp = _ptrs(x_ptrs)
+        py, pyp = _ptrs(y_ptrs)
+        rc = self.lib.ref_kronmult_vbatched_entries(len(x_ptrs), shp, pap, pxp, pyp, wbytes)
         assert rc == 0
 
     def kgemm_batched(self, op, mm, nn, kk, alpha, a_ptrs, ldA, b_ptrs, ldB, beta, c_ptrs, ldC):

@@ -55,6 +55,7 @@
 #include "kgemm_tt_batched.hpp"
 
 #include <omp.h>
+#include <vector>
 
 extern "C" {
 
@@ -172,6 +173,40 @@ int ref_kronmult_vbatched(int d, int const *m, int const *n,
   default: return 1;
   }
   return 0;
+}
+
+// Uneven batch driven through the reference's kronmult{d}_vbatched one entry
+// at a time (batchCount = 1; the reference has no per-entry-shape batch),
+// entries spread over OpenMP threads, each with private workspace.
+// shapes: 13 ints per entry {d, m1, n1, ..., m6, n6}; pA: 6 pointers per
+// entry.  Outputs must not alias between entries.
+int ref_kronmult_vbatched_entries(int nent, int const *shapes, double const *const *pA,
+                                  double **pX, double **pY, size_t Wbytes_per_thread)
+{
+  int bad = 0;
+#pragma omp parallel
+  {
+    std::vector<double> W(Wbytes_per_thread / sizeof(double) + 1);
+#pragma omp for schedule(dynamic, 8)
+    for (int k = 0; k < nent; k++)
+    {
+      int const *s = shapes + 13L * k;
+      int m[6], n[6];
+      for (int l = 0; l < 6; l++)
+      {
+        m[l] = s[1 + 2 * l];
+        n[l] = s[2 + 2 * l];
+      }
+      int rc = ref_kronmult_vbatched(s[0], m, n, pA + 6L * k, pX + k, pY + k, W.data(),
+                                     Wbytes_per_thread, 1);
+      if (rc)
+      {
+#pragma omp atomic write
+        bad = 1;
+      }
+    }
+  }
+  return bad;
 }
 
 // op: 0 = nn, 1 = nt, 2 = tt
