@@ -424,6 +424,32 @@ __device__ void gen_apply_modes(const GenView &v, T *&cur, T *&nxt, const T *As,
       inner *= dims[u];
     const T *Aq         = As + aoff[q]; // Aq[i + j*mq]
     const long long tot = outer * mq * inner;
+    if (PREC != PREC_SPLIT && nq <= 8 && tot < (1LL << 31))
+    {
+      // fibre per thread: its nq inputs are read once, all mq outputs formed
+      // from them (A broadcast from shared memory); 32-bit index math
+      const int in32 = (int)inner, nfib = (int)(outer * inner);
+      for (int f = t; f < nfib; f += GS)
+      {
+        const int o = f / in32, r = f - (f / in32) * in32;
+        const T *src = cur + (o * nq) * in32 + r;
+        T *dst       = nxt + (o * mq) * in32 + r;
+        T x[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+          x[j] = (j < nq) ? src[j * in32] : T(0);
+        for (int i = 0; i < mq; i++)
+        {
+          T z = T(0);
+#pragma unroll
+          for (int j = 0; j < 8; j++)
+            if (j < nq)
+              z = fma(Aq[i + j * mq], x[j], z);
+          dst[i * in32] = z;
+        }
+      }
+    }
+    else
     for (long long idx = t; idx < tot; idx += GS)
     {
       const long long r  = idx % inner;

@@ -40,7 +40,9 @@ struct VDesc
   unsigned char m[6], n[6];
   int mi;               // largest intermediate (elements) of the chosen order
   int mi2;              // huge: phase-2 buffer elements (tile rows x C)
-  unsigned char fwd1, fwd2, pad[2]; // huge: order of phase 1 / phase 2
+  unsigned char fwd1, fwd2;         // huge: order of phase 1 / phase 2
+  unsigned char pad[2];             // huge: [0] warp-parallel phase 1, [1] tail factor
+                                    // elements / 16 (rounded up)
 };
 
 struct VParams
@@ -227,9 +229,20 @@ __global__ void __launch_bounds__(VP_THREADS, 1)
     vp_view(v1, e, q, d - q);
     v1.forward    = e.fwd1;
     const int mi1 = e.mi;
-    for (int h = 0; h < Nhead; h++)
-      vp_group_entry(v1, false, x + (long long)h * Ntail, slot + (long long)h * Mtail, ACC_STORE,
-                     smem, smem + mi1, smem + 2 * mi1, A, ld, tid, VP_THREADS, 0);
+    if (e.pad[0])
+    {
+      // one head block per warp, eight at a time (plan checked the slices fit)
+      const int warp = tid >> 5, lane = tid & 31;
+      const int slice = (2 * mi1 + e.pad[1] * 16 + 1) & ~1;
+      double *b0      = smem + warp * slice;
+      for (int h = warp; h < Nhead; h += VP_WARPS)
+        vp_group_entry(v1, false, x + (long long)h * Ntail, slot + (long long)h * Mtail,
+                       ACC_STORE, b0, b0 + mi1, b0 + 2 * mi1, A, ld, lane, 32, warp);
+    }
+    else
+      for (int h = 0; h < Nhead; h++)
+        vp_group_entry(v1, false, x + (long long)h * Ntail, slot + (long long)h * Mtail,
+                       ACC_STORE, smem, smem + mi1, smem + 2 * mi1, A, ld, tid, VP_THREADS, 0);
     __threadfence_block();
     __syncthreads();
     // phase 2
@@ -329,7 +342,17 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
       e.fwd2 = (unsigned char)lp.v2.forward;
       e.mi2  = lp.v2.max_inter; // rows x C, rounded
       max_slot = std::max(max_slot, lp.slot_elems);
-      smem_huge = std::max(smem_huge, (size_t)std::max(lp.v1.group_elems, lp.v2.group_elems) * 8);
+      size_t need = (size_t)std::max(lp.v1.group_elems, lp.v2.group_elems) * 8;
+      // phase 1 one block per warp when eight slices fit
+      const long long a16   = (lp.v1.asz + 15) / 16;
+      const long long slice = (2LL * lp.v1.max_inter + a16 * 16 + 1) & ~1LL;
+      if (a16 < 256 && (size_t)(VP_WARPS * slice * 8) <= (size_t)(maxsm - 1024))
+      {
+        e.pad[0] = 1;
+        e.pad[1] = (unsigned char)a16;
+        need     = std::max(need, (size_t)(VP_WARPS * slice * 8));
+      }
+      smem_huge = std::max(smem_huge, need);
     }
     e.mi = (c == CLS_HUGE) ? 0 : (int)mi;
     if (c == CLS_HUGE)
