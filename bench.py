@@ -320,6 +320,92 @@ class UnevenBatch(Workload):
         return tot
 
 
+class XbatchedBig(Workload):
+    """d=6, n=8 (262144-element vectors), 1024 entries, outputs drawn with
+    replacement from 716 (aliasing), every A_l from a pool of 32 random 8x8
+    matrices per dimension, N(0,1)/sqrt(8); xbatched layout, atomic mode."""
+
+    def __init__(self, batch=1024, nout=716, d=6, n=8, npool=32, seed=SEED + 5):
+        rng = np.random.default_rng(seed)
+        self.d, self.n, self.batch, self.npool, self.nout = d, n, batch, npool, nout
+        self.L = n ** d
+        self.Apool = rng.standard_normal(n * n * npool * d) / np.sqrt(n)
+        self.aidx = rng.integers(0, npool, size=(batch, d))
+        self.ylist = rng.integers(0, nout, size=batch)
+        self.ndistinct = len(set(self.ylist.tolist()))
+        self.xseed = seed + 1
+        self.name = (f"kronmult6_xbatched n=8 FP64, {batch} entries, outputs drawn from {nout} "
+                     f"({self.ndistinct} distinct), A pool {npool}/dim")
+
+    def flops(self):
+        return float(self.batch) * 2 * self.d * self.n ** (self.d + 1)
+
+    def alg_bytes(self):
+        return 8.0 * (self.L * self.batch + 2 * self.L * self.ndistinct + self.Apool.size)
+
+    def a_offsets(self):
+        l = np.arange(self.d)[None, :]
+        return (self.n * self.n * (l * self.npool + self.aidx)).reshape(-1)
+
+    def setup(self, torch, kb, mode):
+        dev = torch.device("cuda")
+        self.kb = kb
+        g = torch.Generator(device=dev)
+        g.manual_seed(self.xseed)
+        self.dA = torch.from_numpy(self.Apool).to(dev)
+        self.dX = torch.rand(self.L * self.batch, dtype=torch.float64, device=dev,
+                             generator=g) * 2 - 1
+        self.dY = torch.zeros(self.L * self.nout, dtype=torch.float64, device=dev)
+        self.nw = 128
+        self.dW = torch.empty(self.L * self.nw, dtype=torch.float64, device=dev)
+        self.pA = (self.dA.data_ptr() + 8 * torch.from_numpy(self.a_offsets())).to(dev)
+        self.pX = (self.dX.data_ptr() + 8 * self.L * torch.arange(self.batch)).to(dev)
+        self.pY = (self.dY.data_ptr() + 8 * self.L * torch.from_numpy(self.ylist)).to(dev)
+        self.pW = (self.dW.data_ptr() + 8 * self.L * torch.arange(self.nw)).to(dev)
+        self.launches_per_step = 1
+        # e2e host copies: X, Y, A pool and the pointer arrays
+        self.h = {k: v.cpu().pin_memory() for k, v in dict(A=self.dA, X=self.dX, Y=self.dY,
+                                                          pA=self.pA, pX=self.pX,
+                                                          pY=self.pY).items()}
+        self.hYout = torch.empty_like(self.h["Y"]).pin_memory()
+        self.h2d_bytes = sum(v.numel() * v.element_size() for v in self.h.values())
+        self.d2h_bytes = self.hYout.numel() * 8
+
+    def step(self):
+        self.kb.kronmult_xbatched(self.d, self.n, self.pA, self.n, self.pX, self.pY, self.pW,
+                                  subbatch=self.nw // 2)
+
+    def e2e_step(self):
+        self.dA.copy_(self.h["A"], non_blocking=True)
+        self.dX.copy_(self.h["X"], non_blocking=True)
+        self.dY.copy_(self.h["Y"], non_blocking=True)
+        self.pA.copy_(self.h["pA"], non_blocking=True)
+        self.pX.copy_(self.h["pX"], non_blocking=True)
+        self.pY.copy_(self.h["pY"], non_blocking=True)
+        self.step()
+        self.hYout.copy_(self.dY, non_blocking=True)
+
+    def cpu_setup(self, sample_entries):
+        self.cs = min(self.batch, sample_entries, 16)
+        rng = np.random.default_rng(self.xseed)
+        self.cX = rng.uniform(-1, 1, self.L * self.cs)
+        self.cY = np.zeros(self.L * self.nout)
+        self.cW = np.zeros(self.L * self.cs)
+        self.c_ap = (self.Apool.ctypes.data + 8 * self.a_offsets()[: self.cs * self.d]).astype(
+            np.uint64)
+        self.c_xp = (self.cX.ctypes.data + 8 * self.L * np.arange(self.cs)).astype(np.uint64)
+        self.c_yp = (self.cY.ctypes.data + 8 * self.L * self.ylist[: self.cs]).astype(np.uint64)
+        self.c_wp = (self.cW.ctypes.data + 8 * self.L * np.arange(self.cs)).astype(np.uint64)
+        return self.cs
+
+    def cpu_step(self, ref):
+        ref.kronmult_xbatched(self.d, self.n, self.c_ap, self.n, self.c_xp, self.c_yp, self.c_wp,
+                              0)
+
+    def cpu_flops(self):
+        return float(self.cs) * 2 * self.d * self.n ** (self.d + 1)
+
+
 def make_workload(cfg, precision):
     if cfg == 1:
         return BatchedSquare(6, 4, 512, "f64", "uniform")
@@ -330,6 +416,8 @@ def make_workload(cfg, precision):
         return BatchedSquare(6, n, 4096, precision, "normal")
     if cfg == 4:
         return UnevenBatch()
+    if cfg == 5:
+        return XbatchedBig()
     raise SystemExit(f"--config {cfg} not available in this bench")
 
 

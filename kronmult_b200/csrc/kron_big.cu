@@ -96,11 +96,16 @@ struct BigShape
   static constexpr int FPB  = LT / N;
   static constexpr int NB   = (BIG_THREADS / FPB) > 0 ? (BIG_THREADS / FPB) : 1;
   static constexpr int RBUF = ((MMA ? 512 * BIG_WARPS : NB * LT) + 15) / 16 * 16;
-  static constexpr int TBUF = (LH * C + 15) / 16 * 16;
+  // phase 2 on FP64 tensor cores when the head is three 8x8 modes: tiles are
+  // kept transposed, column c at c * PITCH (16-byte aligned columns)
+  static constexpr bool MMA2 = (sizeof(T) == 8) && (N == 8) && (Q == 3);
+  static constexpr int PITCH = 514;
+  static constexpr int TBUF  = ((MMA2 ? C * PITCH : LH * C) + 15) / 16 * 16;
   static constexpr size_t OFF_A    = 0;
   static constexpr size_t OFF_R    = OFF_A + (size_t)ASZ * sizeof(T);           // 2 round buffers
-  static constexpr size_t OFF_TILE = OFF_R + 2 * (size_t)RBUF * sizeof(T);      // 2 tile buffers
-  static constexpr size_t SMEM     = OFF_TILE + 2 * (size_t)TBUF * sizeof(T);
+  // the tensor-core phases use one round and one tile buffer, the others two
+  static constexpr size_t OFF_TILE = OFF_R + (MMA ? 1 : 2) * (size_t)RBUF * sizeof(T);
+  static constexpr size_t SMEM     = OFF_TILE + (MMA2 ? 1 : 2) * (size_t)TBUF * sizeof(T);
 };
 
 template <typename T>
@@ -312,6 +317,101 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
     cluster_sync_all(); // W of this entry is complete
 
     // ---------------- phase 2: head modes on column tiles [tb, te)
+    if constexpr (S::MMA2)
+    {
+      constexpr int PITCH = S::PITCH;
+      const int g = lane >> 2, t = lane & 3;
+      double *tile = reinterpret_cast<double *>(tbuf0);
+      double *xs   = reinterpret_cast<double *>(rbuf0) + warp * 512; // transpose scratch
+      AFrag8 f;
+      load_afrag8(f, reinterpret_cast<const double *>(en.A[0]), en.ld[0],
+                  reinterpret_cast<const double *>(en.A[1]), en.ld[1],
+                  reinterpret_cast<const double *>(en.A[2]), en.ld[2], g, t);
+      const double *wd = reinterpret_cast<const double *>(w);
+      double *yd       = reinterpret_cast<double *>(en.y);
+      for (int tt = tb; tt < te; ++tt)
+      {
+        const int c0 = tt * C, cc = min(C, LT - c0);
+        // W rows -> transposed tile (column c contiguous), loads batched
+        constexpr int B = 8;
+        for (int q0 = tid; q0 < LH * C; q0 += BIG_THREADS * B)
+        {
+          double vals[B];
+#pragma unroll
+          for (int b = 0; b < B; b++)
+          {
+            const int q = q0 + b * BIG_THREADS;
+            const int h = q / C, c = q - (q / C) * C;
+            vals[b] = (q < LH * C && c < cc) ? wd[(long long)h * LT + c0 + c] : 0.0;
+          }
+#pragma unroll
+          for (int b = 0; b < B; b++)
+          {
+            const int q = q0 + b * BIG_THREADS;
+            if (q < LH * C)
+            {
+              const int h = q / C, c = q - (q / C) * C;
+              tile[c * PITCH + h] = vals[b];
+            }
+          }
+        }
+        __syncthreads();
+        // each warp: kron(A_1, A_2, A_3) on whole columns
+        for (int c = warp; c < cc; c += BIG_WARPS)
+        {
+          double *col = tile + c * PITCH;
+          double v[8][2], acc[8][2];
+#pragma unroll
+          for (int q = 0; q < 8; q++)
+          {
+            const double2 u = *reinterpret_cast<const double2 *>(col + q * 64 + g * 8 + 2 * t);
+            v[q][0]   = u.x;
+            v[q][1]   = u.y;
+            acc[q][0] = acc[q][1] = 0.0;
+          }
+          kron8x3_tile(v, acc, f, xs, g, t);
+          __syncwarp();
+          // result element (i0 = 2t+p, i1 = q, i2 = g) stored at i1*64 + i2*8 + i0
+#pragma unroll
+          for (int q = 0; q < 8; q++)
+            *reinterpret_cast<double2 *>(col + q * 64 + g * 8 + 2 * t) =
+                make_double2(acc[q][0], acc[q][1]);
+        }
+        __syncthreads();
+        // tile rows into y, loads batched ahead of stores
+        for (int q0 = tid; q0 < LH * C; q0 += BIG_THREADS * B)
+        {
+          double old[B];
+          if (p.accum != ACC_ATOMIC)
+#pragma unroll
+            for (int b = 0; b < B; b++)
+            {
+              const int q = q0 + b * BIG_THREADS;
+              const int i = q / C, c = q - (q / C) * C;
+              if (q < LH * C && c < cc)
+                old[b] = yd[(long long)i * LT + c0 + c];
+            }
+#pragma unroll
+          for (int b = 0; b < B; b++)
+          {
+            const int q = q0 + b * BIG_THREADS;
+            const int i = q / C, c = q - (q / C) * C;
+            if (q < LH * C && c < cc)
+            {
+              double *dst = yd + (long long)i * LT + c0 + c;
+              const int pos  = ((i >> 3) & 7) * 64 + (i & 7) * 8 + (i >> 6);
+              const double r = tile[c * PITCH + pos];
+              if (p.accum == ACC_ATOMIC)
+                red_add(dst, r);
+              else
+                *dst = old[b] + r;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    else
     {
       auto issue_tile = [&](int tt, T *buf) {
         const int c0 = tt * C, cc = min(C, LT - c0);

@@ -15,8 +15,9 @@
 // group holding mode d next, the middle groups last; when the last pass's
 // stride is at least 16 elements it adds straight into y with coalesced
 // accesses, otherwise a final coalesced sweep does.  For power-of-two n the
-// work buffer is XOR-swizzled within 128-byte rows (row r permutes its
-// elements by r & 15, plus bit 4 from r & 8 for 4-byte elements), which a
+// work buffer is XOR-swizzled within 128-byte rows (8-byte elements: row r
+// permutes its elements by r & 15; 4-byte elements: whole 16-byte chunks by
+// (r & 3) | ((r >> 1) & 4), so contiguous fibres move as float4), which a
 // bank model shows conflict free for every pass.
 //
 // Every mbarrier wait is bounded; on time-out the block records 1 in the
@@ -53,8 +54,11 @@ __device__ __forceinline__ int swz(int e)
     }
     else
     {
+      // 4-byte elements: whole 16-byte chunks are permuted (chunk index XOR
+      // row & 3, and XOR 4 for rows with bit 3 set), so contiguous fibres can
+      // move as float4 while strided passes stay conflict free
       const int row = e >> 5;
-      return e ^ ((row & 15) | ((row & 8) << 1));
+      return e ^ (((row & 3) | ((row >> 1) & 4)) << 2);
     }
   }
   else
@@ -118,6 +122,8 @@ __device__ __forceinline__ void bulk_reduce_add(T *y, const T *src, unsigned byt
 }
 
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// all but the most recent bulk group have finished reading shared memory
+__device__ __forceinline__ void bulk_wait_read_but_last() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 template <typename T>
@@ -168,12 +174,29 @@ __device__ __forceinline__ void pipe_pass(const T *src, T *dst, const T *As, T *
   {
     const int o = f / S, r = f - (f / S) * S;
     const int base = o * (C * S) + r;
+    constexpr bool VEC4 = (sizeof(T) == 4) && (S == 1) && (C % 4 == 0) && (N == 4);
     T v[C];
-#pragma unroll
-    for (int c = 0; c < C; c++)
+    if constexpr (VEC4)
     {
-      const int e = base + c * S;
-      v[c]        = SRC_STAGE ? src[e] : src[swz<T, N>(e)];
+#pragma unroll
+      for (int c = 0; c < C; c += 4)
+      {
+        const int e = base + c;
+        const float4 u = *reinterpret_cast<const float4 *>(src + (SRC_STAGE ? e : swz<T, N>(e)));
+        v[c] = u.x;
+        v[c + 1] = u.y;
+        v[c + 2] = u.z;
+        v[c + 3] = u.w;
+      }
+    }
+    else
+    {
+#pragma unroll
+      for (int c = 0; c < C; c++)
+      {
+        const int e = base + c * S;
+        v[c]        = SRC_STAGE ? src[e] : src[swz<T, N>(e)];
+      }
     }
     // apply the group's factors, fastest mode (a+k-1) first
 #pragma unroll
@@ -198,7 +221,17 @@ __device__ __forceinline__ void pipe_pass(const T *src, T *dst, const T *As, T *
       for (int c = 0; c < C; c++)
         v[c] = w[c];
     }
-    if constexpr (DIRECT)
+    if constexpr (VEC4)
+    {
+#pragma unroll
+      for (int c = 0; c < C; c += 4)
+      {
+        const int e = base + c;
+        *reinterpret_cast<float4 *>(dst + (DIRECT ? e : swz<T, N>(e))) =
+            make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+      }
+    }
+    else if constexpr (DIRECT)
     {
       // final pass: plain (unswizzled) layout into the output stage
 #pragma unroll
@@ -244,8 +277,16 @@ __device__ __forceinline__ void middle_passes(T *work, const T *As, int tid)
   }
 }
 
+// blocks per SM the kernel is compiled for: the 4-byte path moves half the
+// bytes per entry, so more blocks hide its per-entry fixed costs
+template <typename T>
+struct PipeOcc
+{
+  static constexpr int value = sizeof(T) == 4 ? 3 : 2;
+};
+
 template <typename T, int D, int N>
-__global__ void __launch_bounds__(PIPE_THREADS, 2)
+__global__ void __launch_bounds__(PIPE_THREADS, PipeOcc<T>::value)
     kron_pipe_kernel(const __grid_constant__ Params p, int nstage)
 {
   using Lay = PipeLayout<T, D, N>;
@@ -299,6 +340,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, 2)
     for (int i = 0; i < ahead; i++)
       issue(eb + i, i);
   unsigned phases = 0; // bit s = parity to wait for on stage s
+  int pending_e = -1, pending_s = 0; // refill deferred to the next iteration
 
   for (int e = eb; e < ee; ++e)
   {
@@ -399,15 +441,38 @@ __global__ void __launch_bounds__(PIPE_THREADS, 2)
       }
       __syncthreads();
     }
-    // refill the stage with position e + nstage once the reduce has read it
-    if (tid == 0 && e + nstage < ee)
+    // With three or more stages, refill one iteration late: the previous
+    // entry's stage is refilled once its reduce has read it (all bulk groups
+    // but this entry's), so no thread waits on the reduce just issued.  With
+    // two stages that would leave nothing in flight, so refill at once.
+    if (tid == 0)
     {
-      bulk_wait_read();
-      issue(e + nstage, s);
+      if (nstage >= 3)
+      {
+        if (pending_e >= 0)
+        {
+          if (bulk)
+            bulk_wait_read_but_last();
+          else
+            bulk_wait_read();
+          issue(pending_e, pending_s);
+        }
+        pending_e = (e + nstage < ee) ? e + nstage : -1;
+        pending_s = s;
+      }
+      else if (e + nstage < ee)
+      {
+        bulk_wait_read();
+        issue(e + nstage, s);
+      }
     }
   }
   if (tid == 0)
+  {
+    if (pending_e >= 0) // nothing left to compute; no refill needed
+      pending_e = -1;
     bulk_wait_all();
+  }
 }
 
 template <typename T, int D, int N>
@@ -416,11 +481,17 @@ int launch_pipe_t(Params p, cudaStream_t stream)
   using Lay            = PipeLayout<T, D, N>;
   const void *fn       = reinterpret_cast<const void *>(&kron_pipe_kernel<T, D, N>);
   const int maxsm      = device_info().max_smem_optin;
-  // two blocks per SM when two stages each still fit, else one block
-  const long long per2 = (long long)device_info().smem_per_sm / 2 - 1024;
-  int ns = (int)std::min<long long>(MAX_STAGES, (per2 - (long long)Lay::STAGE0) /
-                                                    (long long)Lay::STAGE_BYTES);
-  int per_sm = 2;
+  // PipeOcc blocks per SM when two stages each still fit, else one block
+  int per_sm = PipeOcc<T>::value;
+  int ns     = 0;
+  for (; per_sm >= 2; --per_sm)
+  {
+    const long long budget = (long long)device_info().smem_per_sm / per_sm - 1024;
+    ns = (int)std::min<long long>(MAX_STAGES, (budget - (long long)Lay::STAGE0) /
+                                                  (long long)Lay::STAGE_BYTES);
+    if (ns >= 2)
+      break;
+  }
   if (ns < 2)
   {
     per_sm = 1;
