@@ -431,16 +431,32 @@ def read_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def read_profile_traffic(config):
+def profile_key(args):
+    """Key of a workload in the committed ncu summaries: `cfgN` for the
+    default precision, mode and size, with `-f32`, `-split`, `-segmented`,
+    `-nK` appended for the variants."""
+    key = f"cfg{args.config}"
+    if args.precision != "f64":
+        key += f"-{args.precision}"
+    if args.mode != "atomic":
+        key += f"-{args.mode}"
+    n = os.environ.get("KRON_BENCH_N")
+    if args.config == 3 and n and n != "4":
+        key += f"-n{n}"
+    return key
+
+
+def read_profile_traffic(key):
     """Per-launch DRAM traffic of the dominant kernel from the committed ncu
-    summary (profiles/*.md line `traffic_bytes_per_launch[cfgN]: <bytes>`)."""
+    summary (profiles/*.md line `traffic_bytes_per_launch[<key>]: <bytes>`)."""
     import glob
     import re
 
-    for p in glob.glob(os.path.join(ROOT, "profiles", "*.md")):
+    for p in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
         with open(p) as f:
             for line in f:
-                m = re.match(rf"\s*traffic_bytes_per_launch\[cfg{config}\]:\s*([0-9.eE+]+)", line)
+                m = re.match(rf"\s*traffic_bytes_per_launch\[{re.escape(key)}\]:\s*([0-9.eE+]+)",
+                             line)
                 if m:
                     return float(m.group(1)), os.path.relpath(p, ROOT)
     return None, None
@@ -643,7 +659,7 @@ def run_ours(args, world, rank, local):
         value = world * flops * args.steps / sec / 1e9
         gbs = wl.alg_bytes() * args.steps / sec / 1e9
         per_launch_s = sec / (args.steps * wl.launches_per_step)
-        traffic, tsrc = read_profile_traffic(args.config)
+        traffic, tsrc = read_profile_traffic(profile_key(args))
         if args.config == 2 or args.config == 5:
             fp64 = measure_fp64_peak(torch)
             roof = {"bound": "tensor", "achieved": round(flops / wl.launches_per_step /
