@@ -2,26 +2,31 @@
 // (4 KB .. 64 KB per entry): the HBM-bound regime of kronmult{d}_batched
 // (e.g. d = 6, n = 4, 32 KB vectors in FP64).
 //
-// One persistent 256-thread block per SM owns a balanced contiguous range
-// of entries.  Each entry's x vector and its A_1..A_d block are brought into
-// a ring of shared-memory stages by TMA bulk copies (cp.async.bulk, one
-// elected thread, mbarrier completion) several entries ahead, and y is
-// prefetched into L2 at the same time, so HBM streams while the block
-// computes.  The d mode products run as ceil(d/k) register-blocked passes:
-// a thread loads a fibre of n^k elements spanning k consecutive modes,
-// applies those k factors from registers (k = 2, 2, 1 for n = 3, 4, 5)
-// and writes the fibre back.  Pass order: the group holding mode 1 first
-// (reading the TMA stage, consecutive lanes on consecutive addresses), the
-// group holding mode d next, the middle groups last; when the last pass's
-// stride is at least 16 elements it adds straight into y with coalesced
-// accesses, otherwise a final coalesced sweep does.  For power-of-two n the
-// work buffer is XOR-swizzled within 128-byte rows (8-byte elements: row r
-// permutes its elements by r & 15; 4-byte elements: whole 16-byte chunks by
-// (r & 3) | ((r >> 1) & 4), so contiguous fibres move as float4), which a
-// bank model shows conflict free for every pass.
+// Persistent 256-thread blocks (2 per SM in FP64, 4 in FP32) each own a
+// balanced contiguous range of entries.  Each entry's x vector and its
+// A_1..A_d block are brought into a ring of shared-memory stages by TMA bulk
+// copies (cp.async.bulk, one elected thread, mbarrier completion) ahead of
+// use, and y is prefetched into L2 at the same time, so HBM streams while the
+// block computes.  The d mode products run as ceil(d/k) register-blocked
+// passes: a thread loads a fibre of n^k elements spanning k consecutive
+// modes, applies those k factors from registers (k = 2, 2, 1 for n = 3, 4, 5)
+// and writes the fibre back.  Pass order: group 0 first (reading the stage,
+// consecutive lanes on consecutive addresses), the last group next, the
+// middle groups last; the final pass writes the result, unswizzled, into the
+// entry's stage and one TMA bulk reduce-add adds it into y.  The stage is
+// refilled after the next entry's first pass, when the reduce has read it.
+//
+// For n = 4 the work buffer is XOR-swizzled within 128-byte rows (8-byte
+// elements: row r permutes its elements by r & 15; 4-byte elements: whole
+// 16-byte chunks by (r & 3) | ((r >> 1) & 4), so contiguous fibres move as
+// float4), which a bank model shows conflict free for every pass.  Both
+// swizzles are linear over XOR, so a fibre's element addresses are its base
+// address XOR compile-time constants.  FP32 with n = 4 computes with packed
+// fma.rn.f32x2 on factor layouts prepared once per entry.
 //
 // Every mbarrier wait is bounded; on time-out the block records 1 in the
-// library's device status word (kron_device_status) and leaves.
+// library's device status word (kron_device_status), lets the copies it
+// started land (bounded) and leaves.
 #include <cstdint>
 
 #include "kron_launch.h"
@@ -31,6 +36,12 @@ namespace kron {
 __device__ int g_device_status = 0;
 
 namespace {
+
+// FP32 blocks per SM (compile time; 4 measured best for d = 6, n = 4: more
+// resident warps hide the shared-memory latency of the passes)
+#ifndef KRON_PIPE_F32_BLOCKS
+#define KRON_PIPE_F32_BLOCKS 4
+#endif
 
 constexpr int PIPE_THREADS = 256;
 constexpr int MAX_STAGES   = 6;
@@ -110,6 +121,7 @@ template <typename T>
 __device__ __forceinline__ void bulk_reduce_add(T *y, const T *src, unsigned bytes)
 {
   unsigned s = (unsigned)__cvta_generic_to_shared(src);
+
   if constexpr (sizeof(T) == 8)
     asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.add.f64 [%0], [%1], %2;" ::"l"(y),
                  "r"(s), "r"(bytes)
@@ -122,8 +134,6 @@ __device__ __forceinline__ void bulk_reduce_add(T *y, const T *src, unsigned byt
 }
 
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-// all but the most recent bulk group have finished reading shared memory
-__device__ __forceinline__ void bulk_wait_read_but_last() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 template <typename T>
@@ -133,47 +143,107 @@ __device__ __forceinline__ bool tma_ok(const void *ptr, long long bytes)
          bytes < (1LL << 20);
 }
 
-// Stage layout in shared memory (bytes):
+// Stage layout in shared memory (bytes; every region 16-byte aligned):
 //   [0, 64)                     mbarriers (MAX_STAGES x 8)
-//   [128, 128 + L*sz)           work buffer (swizzled)
-//   [.., + ASZ*sz)              A of the entry being computed
-//   then per stage: x (L*sz) and A (ASZ*sz), 16-byte aligned
+//   [64, 64 + 4*MAX_STAGES)     per-stage operand flags (META_*)
+//   [128, 128 + LB)             work buffer (swizzled)
+//   [.., + AREG)                A of the entry being computed, in the
+//                               layouts the packed FP32 passes read
+//   then per stage: x (LB bytes) and A (AB bytes)
 template <typename T, int D, int N>
 struct PipeLayout
 {
   static constexpr int L        = cpow(N, D);
   static constexpr int ASZ      = D * N * N;
-  static constexpr int ASZ_PAD  = (ASZ + 15) / 16 * 16;
+  static constexpr size_t LB    = ((size_t)L * sizeof(T) + 15) / 16 * 16;
+  static constexpr size_t AB    = ((size_t)ASZ * sizeof(T) + 15) / 16 * 16;
+  // packed FP32: row-major factors (16 floats per mode) + duplicated pairs
+  // (32 floats per mode)
+  static constexpr bool PACKED  = sizeof(T) == 4 && N == 4;
+  static constexpr size_t AREG  = PACKED ? (size_t)D * 48 * sizeof(float) : 0;
   static constexpr size_t WORK  = 128;
-  static constexpr size_t ACUR  = WORK + (size_t)L * sizeof(T);
-  static constexpr size_t STAGE0 = ACUR + (size_t)ASZ_PAD * sizeof(T);
-  static constexpr size_t STAGE_BYTES = ((size_t)L + ASZ_PAD) * sizeof(T);
+  static constexpr size_t ACUR  = WORK + LB;
+  static constexpr size_t STAGE0 = ACUR + AREG;
+  static constexpr size_t STAGE_BYTES = LB + AB;
   static size_t bytes(int ns) { return STAGE0 + ns * STAGE_BYTES; }
 };
 
-// One register-blocked pass over the modes [a, a+k): SRC/DST select the
-// stage (unswizzled) / work buffer (swizzled) / y (global, DIRECT).
-template <typename T, int D, int N, int a, int k, bool SRC_STAGE, bool DIRECT>
-__device__ __forceinline__ void pipe_pass(const T *src, T *dst, const T *As, T *y, int accum,
-                                          int tid)
+// flags the issuing thread records per stage
+constexpr int META_X_TMA  = 1; // x arrived by bulk copy
+constexpr int META_A_TMA  = 2; // A_1..A_d arrived by bulk copy (contiguous)
+constexpr int META_Y_BULK = 4; // y takes the bulk reduce-add
+
+// Offset of element base + kk of a fibre.  In a swizzled buffer the XOR
+// swizzle is linear over GF(2) and base, kk occupy disjoint bits (n = 4:
+// base = o*C*S + r with r < S, kk = c*S < C*S), so
+// swz(base + kk) = swz(base) ^ swz(kk) with swz(kk) a compile-time constant.
+template <typename T, int N, bool SWZ>
+__device__ __forceinline__ int fib_off(int sb, int kk)
+{
+  if constexpr (SWZ && N == 4)
+    return sb ^ swz<T, N>(kk);
+  else
+    return sb + kk;
+}
+
+// the k factors of a group, Ar[m][i][j] = A_{a+m}(i, j), from column-major
+// storage (16-byte aligned for n = 4: one vector load per column)
+template <typename T, int N, int k>
+__device__ __forceinline__ void load_factors(const T *As, T (&Ar)[k][N][N])
+{
+#pragma unroll
+  for (int m = 0; m < k; m++)
+#pragma unroll
+    for (int j = 0; j < N; j++)
+    {
+      if constexpr (N == 4 && sizeof(T) == 8)
+      {
+        const double2 u0 = *reinterpret_cast<const double2 *>(As + m * 16 + 4 * j);
+        const double2 u1 = *reinterpret_cast<const double2 *>(As + m * 16 + 4 * j + 2);
+        Ar[m][0][j] = u0.x;
+        Ar[m][1][j] = u0.y;
+        Ar[m][2][j] = u1.x;
+        Ar[m][3][j] = u1.y;
+      }
+      else if constexpr (N == 4 && sizeof(T) == 4)
+      {
+        const float4 u = *reinterpret_cast<const float4 *>(As + m * 16 + 4 * j);
+        Ar[m][0][j] = u.x;
+        Ar[m][1][j] = u.y;
+        Ar[m][2][j] = u.z;
+        Ar[m][3][j] = u.w;
+      }
+      else
+      {
+#pragma unroll
+        for (int i = 0; i < N; i++)
+          Ar[m][i][j] = As[m * N * N + i + j * N];
+      }
+    }
+}
+
+// destinations of a pass
+constexpr int DST_WORK  = 0; // work buffer (swizzled)
+constexpr int DST_STAGE = 1; // stage buffer (plain layout)
+
+// One register-blocked pass over the modes [a, a+k): the source is the
+// stage (plain layout) or the work buffer (swizzled).  As points at A_1
+// (column-major, n x n per mode).
+template <typename T, int D, int N, int a, int k, bool SRC_STAGE, int DST>
+__device__ __forceinline__ void pipe_pass(const T *src, T *dst, const T *As, int tid)
 {
   constexpr int S = cpow(N, D - a - k); // stride of the group's last mode
   constexpr int C = cpow(N, k);
   constexpr int F = cpow(N, D) / C;
-  // factors of the group in registers: Ar[m][i][j] = A_{a+m}(i, j)
   T Ar[k][N][N];
-#pragma unroll
-  for (int m = 0; m < k; m++)
-#pragma unroll
-    for (int i = 0; i < N; i++)
-#pragma unroll
-      for (int j = 0; j < N; j++)
-        Ar[m][i][j] = As[(a + m) * N * N + i + j * N];
+  load_factors<T, N, k>(As + a * N * N, Ar);
 
   for (int f = tid; f < F; f += PIPE_THREADS)
   {
     const int o = f / S, r = f - (f / S) * S;
     const int base = o * (C * S) + r;
+    const int sbs  = SRC_STAGE ? base : swz<T, N>(base);
+    const int sbd  = DST == DST_WORK ? swz<T, N>(base) : base;
     constexpr bool VEC4 = (sizeof(T) == 4) && (S == 1) && (C % 4 == 0) && (N == 4);
     T v[C];
     if constexpr (VEC4)
@@ -181,8 +251,7 @@ __device__ __forceinline__ void pipe_pass(const T *src, T *dst, const T *As, T *
 #pragma unroll
       for (int c = 0; c < C; c += 4)
       {
-        const int e = base + c;
-        const float4 u = *reinterpret_cast<const float4 *>(src + (SRC_STAGE ? e : swz<T, N>(e)));
+        const float4 u = *reinterpret_cast<const float4 *>(src + fib_off<T, N, !SRC_STAGE>(sbs, c));
         v[c] = u.x;
         v[c + 1] = u.y;
         v[c + 2] = u.z;
@@ -193,17 +262,12 @@ __device__ __forceinline__ void pipe_pass(const T *src, T *dst, const T *As, T *
     {
 #pragma unroll
       for (int c = 0; c < C; c++)
-      {
-        const int e = base + c * S;
-        v[c]        = SRC_STAGE ? src[e] : src[swz<T, N>(e)];
-      }
+        v[c] = src[fib_off<T, N, !SRC_STAGE>(sbs, c * S)];
     }
     // apply the group's factors, fastest mode (a+k-1) first
 #pragma unroll
     for (int m = k - 1; m >= 0; m--)
     {
-      constexpr int dummy = 0;
-      (void)dummy;
       const int inner = cpow(N, k - 1 - m); // stride of mode a+m inside the fibre
       T w[C];
 #pragma unroll
@@ -225,29 +289,187 @@ __device__ __forceinline__ void pipe_pass(const T *src, T *dst, const T *As, T *
     {
 #pragma unroll
       for (int c = 0; c < C; c += 4)
-      {
-        const int e = base + c;
-        *reinterpret_cast<float4 *>(dst + (DIRECT ? e : swz<T, N>(e))) =
+        *reinterpret_cast<float4 *>(dst + fib_off<T, N, DST == DST_WORK>(sbd, c)) =
             make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
-      }
-    }
-    else if constexpr (DIRECT)
-    {
-      // final pass: plain (unswizzled) layout into the output stage
-#pragma unroll
-      for (int c = 0; c < C; c++)
-        dst[base + c * S] = v[c];
     }
     else
     {
 #pragma unroll
       for (int c = 0; c < C; c++)
-        dst[swz<T, N>(base + c * S)] = v[c];
+        dst[fib_off<T, N, DST == DST_WORK>(sbd, c * S)] = v[c];
     }
   }
 }
 
-// Passes in order: group 0, then the last group, then the middle groups.
+// ---- packed FP32 (fma.rn.f32x2) passes for n = 4 ----
+typedef unsigned long long f2_t; // two floats in one 64-bit register pair
+
+__device__ __forceinline__ f2_t pk2(float x, float y)
+{
+  f2_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
+  return r;
+}
+__device__ __forceinline__ void upk2(f2_t r, float &x, float &y)
+{
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(r));
+}
+__device__ __forceinline__ float hsum2(f2_t r)
+{
+  float x, y;
+  upk2(r, x, y);
+  return x + y;
+}
+__device__ __forceinline__ f2_t mul2(f2_t a, f2_t b)
+{
+  f2_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2_t fma2(f2_t a, f2_t b, f2_t c)
+{
+  f2_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+// Factor layouts for the packed passes, built once per entry:
+//   arow[l*16 + 4i + j]  = A_l(i, j)            (row major)
+//   adup[l*16 + 4i + j]  = {A_l(i, j), A_l(i, j)}
+// A mode in the fast position of its pass contracts horizontally
+// (pairs {A(i,2h), A(i,2h+1)} times pairs of consecutive inputs, then one
+// add); a mode in the slow position scales pairs of independent columns by
+// a duplicated coefficient.
+__device__ __forceinline__ void prep_packed(const float *Acol, float *areg, int D, int tid)
+{
+  float *arow = areg;
+  float2 *adup = reinterpret_cast<float2 *>(areg + D * 16);
+  for (int t = tid; t < D * 16; t += PIPE_THREADS)
+  {
+    const int l = t >> 4, i = t & 3, j = (t >> 2) & 3; // t = l*16 + i + 4j
+    const float val = Acol[t];
+    arow[l * 16 + 4 * i + j] = val;
+    adup[l * 16 + 4 * i + j] = make_float2(val, val);
+  }
+}
+
+// fibre of 4 consecutive-mode elements v[4q + j] (q = slow index, j = fast):
+// w[4q + i] = sum_j A(i, j) v[4q + j] with V[2q + h] = {v[4q+2h], v[4q+2h+1]}
+template <int Q>
+__device__ __forceinline__ void fast_mode(const float *arow, const f2_t (&V)[2 * Q], float (&w)[4 * Q])
+{
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+  {
+    const ulonglong2 P = *reinterpret_cast<const ulonglong2 *>(arow + 4 * i);
+#pragma unroll
+    for (int q = 0; q < Q; q++)
+      w[4 * q + i] = hsum2(fma2(P.y, V[2 * q + 1], mul2(P.x, V[2 * q])));
+  }
+}
+
+template <int D, int a, int k, bool SRC_STAGE, int DST>
+__device__ __forceinline__ void pipe_pass_packed(const float *src, float *dst, const float *areg,
+                                                 int tid)
+{
+  constexpr int N = 4;
+  constexpr int S = cpow(N, D - a - k);
+  constexpr int C = cpow(N, k);
+  constexpr int F = cpow(N, D) / C;
+  static_assert(k == 1 || k == 2, "packed passes cover one or two modes");
+  static_assert(k == 2 || S == 1, "a one-mode packed pass is the last (contiguous) group");
+  const float *arow = areg + (a + k - 1) * 16; // fast mode a+k-1
+  const f2_t *adup  = reinterpret_cast<const f2_t *>(areg + D * 16) + a * 16; // slow mode a
+
+  for (int f = tid; f < F; f += PIPE_THREADS)
+  {
+    const int o = f / S, r = f - (f / S) * S;
+    const int base = o * (C * S) + r;
+    const int sbs  = SRC_STAGE ? base : swz<float, N>(base);
+    const int sbd  = DST == DST_WORK ? swz<float, N>(base) : base;
+    constexpr int Q = C / 4;
+    f2_t V[2 * Q];
+    if constexpr (S == 1)
+    {
+#pragma unroll
+      for (int q = 0; q < Q; q++)
+      {
+        const ulonglong2 u =
+            *reinterpret_cast<const ulonglong2 *>(src + fib_off<float, N, !SRC_STAGE>(sbs, 4 * q));
+        V[2 * q]     = u.x;
+        V[2 * q + 1] = u.y;
+      }
+    }
+    else
+    {
+#pragma unroll
+      for (int c = 0; c < C; c += 2)
+        V[c / 2] = pk2(src[fib_off<float, N, !SRC_STAGE>(sbs, c * S)],
+                       src[fib_off<float, N, !SRC_STAGE>(sbs, (c + 1) * S)]);
+    }
+    float w[C];
+    fast_mode<Q>(arow, V, w);
+    f2_t O[2 * Q];
+    if constexpr (k == 1)
+    {
+      O[0] = pk2(w[0], w[1]);
+      O[1] = pk2(w[2], w[3]);
+    }
+    else
+    {
+      // slow mode a: out[4q' + t] = sum_j A_a(q', j) w[4j + t], t in pairs
+      f2_t W[8];
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+      {
+        W[2 * j]     = pk2(w[4 * j], w[4 * j + 1]);
+        W[2 * j + 1] = pk2(w[4 * j + 2], w[4 * j + 3]);
+      }
+#pragma unroll
+      for (int qq = 0; qq < 4; qq++)
+      {
+        const ulonglong2 D01 = *reinterpret_cast<const ulonglong2 *>(adup + 4 * qq);
+        const ulonglong2 D23 = *reinterpret_cast<const ulonglong2 *>(adup + 4 * qq + 2);
+#pragma unroll
+        for (int tp = 0; tp < 2; tp++)
+          O[2 * qq + tp] =
+              fma2(D23.y, W[6 + tp], fma2(D23.x, W[4 + tp], fma2(D01.y, W[2 + tp], mul2(D01.x, W[tp]))));
+      }
+    }
+    if constexpr (S == 1)
+    {
+#pragma unroll
+      for (int q = 0; q < Q; q++)
+        *reinterpret_cast<ulonglong2 *>(dst + fib_off<float, N, DST == DST_WORK>(sbd, 4 * q)) =
+            make_ulonglong2(O[2 * q], O[2 * q + 1]);
+    }
+    else
+    {
+#pragma unroll
+      for (int c = 0; c < C; c += 2)
+      {
+        float x0, x1;
+        upk2(O[c / 2], x0, x1);
+        dst[fib_off<float, N, DST == DST_WORK>(sbd, c * S)]       = x0;
+        dst[fib_off<float, N, DST == DST_WORK>(sbd, (c + 1) * S)] = x1;
+      }
+    }
+  }
+}
+
+// dispatch one pass to the packed or the scalar form
+template <typename T, int D, int N, int a, int k, bool SRC_STAGE, int DST>
+__device__ __forceinline__ void run_pass(const T *src, T *dst, const T *As, int tid)
+{
+  if constexpr (PipeLayout<T, D, N>::PACKED)
+    pipe_pass_packed<D, a, k, SRC_STAGE, DST>(src, dst, As, tid);
+  else
+    pipe_pass<T, D, N, a, k, SRC_STAGE, DST>(src, dst, As, tid);
+}
+
+// Passes in order: group 0 (reads the stage), then the last group, then the
+// middle groups; the final pass writes the result into the stage for one
+// bulk reduce-add.
 template <typename T, int D, int N>
 struct PipePlan
 {
@@ -270,7 +492,7 @@ __device__ __forceinline__ void middle_passes(T *work, const T *As, int tid)
     constexpr int a = gi * P::k;
     if constexpr (gi != P::ngroup - 2) // group ngroup-2 is the final pass
     {
-      pipe_pass<T, D, N, a, P::k, false, false>(work, work, As, nullptr, 0, tid);
+      run_pass<T, D, N, a, P::k, false, DST_WORK>(work, work, As, tid);
       __syncthreads();
     }
     middle_passes<T, D, N, gi + 1>(work, As, tid);
@@ -282,7 +504,7 @@ __device__ __forceinline__ void middle_passes(T *work, const T *As, int tid)
 template <typename T>
 struct PipeOcc
 {
-  static constexpr int value = sizeof(T) == 4 ? 3 : 2;
+  static constexpr int value = sizeof(T) == 4 ? KRON_PIPE_F32_BLOCKS : 2;
 };
 
 template <typename T, int D, int N>
@@ -295,10 +517,13 @@ __global__ void __launch_bounds__(PIPE_THREADS, PipeOcc<T>::value)
   constexpr int ASZ = Lay::ASZ;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+  int *meta      = reinterpret_cast<int *>(smem + 64);
   T *work        = reinterpret_cast<T *>(smem + Lay::WORK);
-  T *acur        = reinterpret_cast<T *>(smem + Lay::ACUR);
+  T *areg        = reinterpret_cast<T *>(smem + Lay::ACUR);
   auto stage_x   = [&](int s) { return reinterpret_cast<T *>(smem + Lay::STAGE0 + s * Lay::STAGE_BYTES); };
-  auto stage_a   = [&](int s) { return stage_x(s) + L; };
+  auto stage_a   = [&](int s) {
+    return reinterpret_cast<T *>(smem + Lay::STAGE0 + s * Lay::STAGE_BYTES + Lay::LB);
+  };
   const int tid  = threadIdx.x;
 
   const long long tot = p.eend - p.ebase;
@@ -315,24 +540,29 @@ __global__ void __launch_bounds__(PIPE_THREADS, PipeOcc<T>::value)
   }
   __syncthreads();
 
-  // issue the copies of position e into stage s (thread 0 only)
+  const long long xb = (long long)L * sizeof(T);
+  const long long ab = (long long)ASZ * sizeof(T);
+  unsigned inflight = 0; // thread 0: stages with copies not yet waited for
+  // issue the copies of position e into stage s (thread 0 only) and record
+  // which operands the copies carry
   auto issue = [&](int e, int s) {
     EntryRef<T> en;
     entry_fetch<T>(p, entry_index(p, e), D, en);
-    const long long xb = (long long)L * sizeof(T);
-    const long long ab = (long long)ASZ * sizeof(T);
     const bool a_contig =
         (p.layout == LAYOUT_BATCHED || p.layout == LAYOUT_PBATCHED) && tma_ok<T>(en.A[0], ab);
     const bool x_ok = tma_ok<T>(en.x, xb);
-    unsigned bytes  = (x_ok ? (unsigned)xb : 0u) + (a_contig ? (unsigned)ab : 0u);
+    const bool y_ok = tma_ok<T>(en.y, xb);
+    meta[s] = (x_ok ? META_X_TMA : 0) | (a_contig ? META_A_TMA : 0) | (y_ok ? META_Y_BULK : 0);
+    unsigned bytes = (x_ok ? (unsigned)xb : 0u) + (a_contig ? (unsigned)ab : 0u);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(&bars[s], bytes);
     if (x_ok)
       tma_load(stage_x(s), en.x, (unsigned)xb, &bars[s]);
     if (a_contig)
       tma_load(stage_a(s), en.A[0], (unsigned)ab, &bars[s]);
-    if (tma_ok<T>(en.y, xb))
+    if (y_ok)
       l2_prefetch(en.y, (unsigned)xb);
+    inflight |= 1u << s;
   };
 
   int ahead = min(nstage, ee - eb);
@@ -340,14 +570,14 @@ __global__ void __launch_bounds__(PIPE_THREADS, PipeOcc<T>::value)
     for (int i = 0; i < ahead; i++)
       issue(eb + i, i);
   unsigned phases = 0; // bit s = parity to wait for on stage s
-  int pending_e = -1, pending_s = 0; // refill deferred to the next iteration
+  int pending_e = -1, pending_s = 0; // stage refill waiting for its reduce to read it
 
   for (int e = eb; e < ee; ++e)
   {
     const int s = (e - eb) % nstage;
-    EntryRef<T> en;
-    entry_fetch<T>(p, entry_index(p, e), D, en);
-    // wait for stage s (bounded)
+    // wait for stage s (bounded); the outcome is combined at the barrier
+    // below, after the A preparation (which reads in-bounds shared memory
+    // either way)
     bool done = false;
     for (long long it = 0; it < SPIN_LIMIT; ++it)
       if (mbar_try_wait(&bars[s], (phases >> s) & 1))
@@ -355,68 +585,93 @@ __global__ void __launch_bounds__(PIPE_THREADS, PipeOcc<T>::value)
         done = true;
         break;
       }
+    if (tid == 0 && done)
+      inflight &= ~(1u << s);
+    const int fl = meta[s];
+    T *sx        = stage_x(s);
+    T *sa        = stage_a(s);
+    // operands the bulk copy could not take (block-uniform): plain loads
+    // into the same stage
+    if ((fl & (META_X_TMA | META_A_TMA)) != (META_X_TMA | META_A_TMA))
+    {
+      EntryRef<T> en;
+      entry_fetch<T>(p, entry_index(p, e), D, en);
+      if (!(fl & META_X_TMA))
+        for (int i = tid; i < L; i += PIPE_THREADS)
+          sx[i] = __ldg(en.x + i);
+      if (!(fl & META_A_TMA))
+      {
+#pragma unroll
+        for (int l = 0; l < D; l++)
+          for (int ij = tid; ij < N * N; ij += PIPE_THREADS)
+          {
+            const int j = ij / N, i = ij - j * N;
+            sa[l * N * N + ij] = __ldg(en.A[l] + i + (long long)j * en.ld[l]);
+          }
+      }
+      __syncthreads();
+    }
+    // A for this entry's passes: straight from the stage, or (packed FP32)
+    // in the layouts the packed passes read
+    const T *As = sa;
+    if constexpr (Lay::PACKED)
+    {
+      prep_packed(reinterpret_cast<const float *>(sa), reinterpret_cast<float *>(areg), D, tid);
+      As = areg;
+    }
     if (!__syncthreads_and(done))
     {
       if (tid == 0)
+      {
         atomicExch(&g_device_status, 1);
+        // let the copies this block started land before it leaves (bounded)
+        for (int s2 = 0; s2 < nstage; s2++)
+          if ((inflight >> s2) & 1)
+            for (long long it = 0; it < SPIN_LIMIT; ++it)
+              if (mbar_try_wait(&bars[s2], (phases >> s2) & 1))
+                break;
+        bulk_wait_all();
+      }
       return;
     }
     phases ^= 1u << s;
-    // operands the TMA could not take: plain loads
-    const long long xb = (long long)L * sizeof(T);
-    const long long ab = (long long)ASZ * sizeof(T);
-    T *sx = stage_x(s);
-    if (!tma_ok<T>(en.x, xb))
-      for (int i = tid; i < L; i += PIPE_THREADS)
-        sx[i] = __ldg(en.x + i);
-    const bool a_contig =
-        (p.layout == LAYOUT_BATCHED || p.layout == LAYOUT_PBATCHED) && tma_ok<T>(en.A[0], ab);
-    if (a_contig)
-    {
-      const T *sa = stage_a(s);
-      for (int i = tid; i < ASZ; i += PIPE_THREADS)
-        acur[i] = sa[i];
-    }
-    else
-    {
-#pragma unroll
-      for (int l = 0; l < D; l++)
-        for (int ij = tid; ij < N * N; ij += PIPE_THREADS)
-        {
-          const int j = ij / N, i = ij - j * N;
-          acur[l * N * N + ij] = __ldg(en.A[l] + i + (long long)j * en.ld[l]);
-        }
-    }
-    __syncthreads();
 
     // pass 1: group 0, stage -> work
-    pipe_pass<T, D, N, 0, P::k, true, false>(sx, work, acur, nullptr, 0, tid);
+    run_pass<T, D, N, 0, P::k, true, DST_WORK>(sx, work, As, tid);
     __syncthreads();
+    // the previous entry's reduce was issued a pass ago: refill its stage
+    if (tid == 0 && pending_e >= 0)
+    {
+      bulk_wait_read();
+      issue(pending_e, pending_s);
+      pending_e = -1;
+    }
 
     // remaining passes; the last writes the result, unswizzled, into the
     // (now free) stage buffer
     if constexpr (P::ngroup >= 3)
     {
-      pipe_pass<T, D, N, P::last_a, P::last_k, false, false>(work, work, acur, nullptr, 0, tid);
+      run_pass<T, D, N, P::last_a, P::last_k, false, DST_WORK>(work, work, As, tid);
       __syncthreads();
-      middle_passes<T, D, N, 1>(work, acur, tid);
-      pipe_pass<T, D, N, P::final_a, P::final_k, false, true>(work, sx, acur, nullptr, 0, tid);
+      middle_passes<T, D, N, 1>(work, As, tid);
+      run_pass<T, D, N, P::final_a, P::final_k, false, DST_STAGE>(work, sx, As, tid);
     }
     else
-      pipe_pass<T, D, N, P::last_a, P::last_k, false, true>(work, sx, acur, nullptr, 0, tid);
+      run_pass<T, D, N, P::last_a, P::last_k, false, DST_STAGE>(work, sx, As, tid);
 
     // y += result: one bulk reduce-add by the TMA engine when y allows it
-    const bool bulk = tma_ok<T>(en.y, xb);
+    const bool bulk = (fl & META_Y_BULK) != 0;
     if (bulk)
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (bulk)
     {
       if (tid == 0)
-        bulk_reduce_add(en.y, sx, (unsigned)xb);
+        bulk_reduce_add(entry_y<T>(p, entry_index(p, e)), sx, (unsigned)xb);
     }
     else
     {
+      T *y = entry_y<T>(p, entry_index(p, e));
       constexpr int B = 8;
       for (int i0 = tid; i0 < L; i0 += PIPE_THREADS * B)
       {
@@ -425,7 +680,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PipeOcc<T>::value)
 #pragma unroll
           for (int b = 0; b < B; b++)
             if (i0 + b * PIPE_THREADS < L)
-              yv[b] = en.y[i0 + b * PIPE_THREADS];
+              yv[b] = y[i0 + b * PIPE_THREADS];
 #pragma unroll
         for (int b = 0; b < B; b++)
         {
@@ -433,46 +688,24 @@ __global__ void __launch_bounds__(PIPE_THREADS, PipeOcc<T>::value)
           if (i < L)
           {
             if (p.accum == ACC_ATOMIC)
-              red_add(en.y + i, sx[i]);
+              red_add(y + i, sx[i]);
             else
-              en.y[i] = yv[b] + sx[i];
+              y[i] = yv[b] + sx[i];
           }
         }
       }
       __syncthreads();
     }
-    // With three or more stages, refill one iteration late: the previous
-    // entry's stage is refilled once its reduce has read it (all bulk groups
-    // but this entry's), so no thread waits on the reduce just issued.  With
-    // two stages that would leave nothing in flight, so refill at once.
-    if (tid == 0)
+    // the stage now holds the result; it is refilled after the next
+    // entry's first pass, when the reduce has read it
+    if (tid == 0 && e + nstage < ee)
     {
-      if (nstage >= 3)
-      {
-        if (pending_e >= 0)
-        {
-          if (bulk)
-            bulk_wait_read_but_last();
-          else
-            bulk_wait_read();
-          issue(pending_e, pending_s);
-        }
-        pending_e = (e + nstage < ee) ? e + nstage : -1;
-        pending_s = s;
-      }
-      else if (e + nstage < ee)
-      {
-        bulk_wait_read();
-        issue(e + nstage, s);
-      }
+      pending_e = e + nstage;
+      pending_s = s;
     }
   }
   if (tid == 0)
-  {
-    if (pending_e >= 0) // nothing left to compute; no refill needed
-      pending_e = -1;
     bulk_wait_all();
-  }
 }
 
 template <typename T, int D, int N>

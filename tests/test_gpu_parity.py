@@ -343,6 +343,35 @@ def test_pipelined_layouts(gpu_lib, d, n, layout, offset):
     assert kb.lib().kron_device_status(1) == 0
 
 
+@pytest.mark.parametrize("d,n,prec,batch", [
+    (6, 3, "f64", 1200), (5, 5, "f64", 1200), (4, 5, "f64", 1200), (6, 4, "f64", 1200),
+    (5, 4, "f64", 1200), (6, 4, "f32", 1800), (5, 4, "f32", 1800), (5, 5, "f32", 1800),
+    (6, 5, "f32", 900),
+])
+def test_pipelined_every_stage(gpu_lib, d, n, prec, batch):
+    """Enough entries that every block of the pipelined kernel cycles
+    through all of its stages (odd vector lengths included, whose stage
+    slots are padded to 16 bytes), in FP64 and in FP32."""
+    torch = _torch()
+    rng = np.random.default_rng(1700 + 10 * d + n)
+    L = n ** d
+    A = rng.uniform(-1, 1, n * n * d * batch)
+    X = rng.uniform(-1, 1, L * batch)
+    Y0 = rng.uniform(-1, 1, L * batch)
+    Yref = Y0.copy()
+    oracle.kronmult_batched(d, n, A, X, Yref)
+    if prec == "f64":
+        dY = dev(Y0)
+        kb.kronmult_batched(d, n, dev(A), dev(X), dY)
+        tol = TOL64
+    else:
+        dY = dev(Y0, torch.float32)
+        kb.kronmult_batched_f32(d, n, dev(A, torch.float32), dev(X, torch.float32), dY, None)
+        tol = TOL32
+    assert rel_err(host(dY).astype(np.float64), Yref) <= tol
+    assert kb.lib().kron_device_status(1) == 0
+
+
 @pytest.mark.parametrize("d,n,batch,prec,layout", [
     (6, 7, 3, "f64", "batched"), (6, 8, 2, "f64", "batched"), (5, 8, 5, "f64", "pbatched"),
     (6, 8, 3, "f64", "xbatched"), (6, 7, 2, "f32", "batched"), (6, 8, 2, "f32", "batched"),
