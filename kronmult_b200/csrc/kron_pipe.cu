@@ -22,7 +22,10 @@
 // float4), which a bank model shows conflict free for every pass.  Both
 // swizzles are linear over XOR, so a fibre's element addresses are its base
 // address XOR compile-time constants.  FP32 with n = 4 computes with packed
-// fma.rn.f32x2 on factor layouts prepared once per entry.
+// fma.rn.f32x2 / mul.rn.f32x2 from a row-major copy of the factors made once
+// per entry: each output is two pair products and one add.  For d = 6,
+// n = 4 the last two passes stay inside each warp's slabs and are separated
+// by a warp barrier only.
 //
 // Every mbarrier wait is bounded; on time-out the block records 1 in the
 // library's device status word (kron_device_status), lets the copies it
@@ -143,24 +146,47 @@ __device__ __forceinline__ bool tma_ok(const void *ptr, long long bytes)
          bytes < (1LL << 20);
 }
 
+// Passes in order: group 0 (reads the stage), then the last group, then the
+// middle groups; the final pass writes the result into the stage for one
+// bulk reduce-add.
+template <typename T, int D, int N>
+struct PipePlan
+{
+  static constexpr int k      = GroupK<N>::k;
+  static constexpr int ngroup = (D + k - 1) / k;
+  static constexpr int last_a = (ngroup - 1) * k;
+  static constexpr int last_k = D - last_a;
+  // stride of the pass executed last (a middle group when ngroup >= 3)
+  static constexpr int final_a = ngroup >= 3 ? (ngroup - 2) * k : last_a;
+  static constexpr int final_k = ngroup >= 3 ? k : last_k;
+  static constexpr int final_S = cpow(N, D - final_a - final_k);
+  // d = 6 with two-mode groups: the last-group pass (fibre f = n^2
+  // contiguous elements, inside slab f / n^2) and the final middle pass
+  // (fibre f = o n^2 + r, inside slab o = f / n^2) keep fibre f in the same
+  // slab (fixed i_1, i_2) of n^4 elements; with f = thread index and n^2
+  // dividing the warp size (n = 4), each warp's fibres cover whole slabs,
+  // so a warp reads and writes only its own slabs between the two passes
+  static constexpr bool WARP_LOCAL_TAIL =
+      D == 6 && k == 2 && ngroup == 3 && 32 % (N * N) == 0 && cpow(N, 4) <= PIPE_THREADS;
+};
+
 // Stage layout in shared memory (bytes; every region 16-byte aligned):
 //   [0, 64)                     mbarriers (MAX_STAGES x 8)
 //   [64, 64 + 4*MAX_STAGES)     per-stage operand flags (META_*)
 //   [128, 128 + LB)             work buffer (swizzled)
-//   [.., + AREG)                A of the entry being computed, in the
-//                               layouts the packed FP32 passes read
-//   then per stage: x (LB bytes) and A (AB bytes)
+//   [.., + AREG)                A of the entry being computed, row major
+//                               (packed FP32 passes only)
+//   then per stage: x (LB bytes) and A (AB bytes); the final pass writes the
+//   result over x
 template <typename T, int D, int N>
 struct PipeLayout
 {
   static constexpr int L        = cpow(N, D);
   static constexpr int ASZ      = D * N * N;
+  static constexpr bool PACKED  = sizeof(T) == 4 && N == 4;
   static constexpr size_t LB    = ((size_t)L * sizeof(T) + 15) / 16 * 16;
   static constexpr size_t AB    = ((size_t)ASZ * sizeof(T) + 15) / 16 * 16;
-  // packed FP32: row-major factors (16 floats per mode) + duplicated pairs
-  // (32 floats per mode)
-  static constexpr bool PACKED  = sizeof(T) == 4 && N == 4;
-  static constexpr size_t AREG  = PACKED ? (size_t)D * 48 * sizeof(float) : 0;
+  static constexpr size_t AREG  = PACKED ? (size_t)D * 16 * sizeof(float) : 0;
   static constexpr size_t WORK  = 128;
   static constexpr size_t ACUR  = WORK + LB;
   static constexpr size_t STAGE0 = ACUR + AREG;
@@ -333,23 +359,16 @@ __device__ __forceinline__ f2_t fma2(f2_t a, f2_t b, f2_t c)
   return d;
 }
 
-// Factor layouts for the packed passes, built once per entry:
-//   arow[l*16 + 4i + j]  = A_l(i, j)            (row major)
-//   adup[l*16 + 4i + j]  = {A_l(i, j), A_l(i, j)}
-// A mode in the fast position of its pass contracts horizontally
-// (pairs {A(i,2h), A(i,2h+1)} times pairs of consecutive inputs, then one
-// add); a mode in the slow position scales pairs of independent columns by
-// a duplicated coefficient.
-__device__ __forceinline__ void prep_packed(const float *Acol, float *areg, int D, int tid)
+// Factor layout for the packed passes, built once per entry:
+//   arow[l*16 + 4i + j] = A_l(i, j)   (row major)
+// Both modes of a pass contract horizontally: pairs {A(i,2h), A(i,2h+1)}
+// times pairs of the two inputs they multiply, then one add per output.
+__device__ __forceinline__ void prep_packed(const float *Acol, float *arow, int D, int tid)
 {
-  float *arow = areg;
-  float2 *adup = reinterpret_cast<float2 *>(areg + D * 16);
   for (int t = tid; t < D * 16; t += PIPE_THREADS)
   {
     const int l = t >> 4, i = t & 3, j = (t >> 2) & 3; // t = l*16 + i + 4j
-    const float val = Acol[t];
-    arow[l * 16 + 4 * i + j] = val;
-    adup[l * 16 + 4 * i + j] = make_float2(val, val);
+    arow[l * 16 + 4 * i + j] = Acol[t];
   }
 }
 
@@ -379,7 +398,7 @@ __device__ __forceinline__ void pipe_pass_packed(const float *src, float *dst, c
   static_assert(k == 1 || k == 2, "packed passes cover one or two modes");
   static_assert(k == 2 || S == 1, "a one-mode packed pass is the last (contiguous) group");
   const float *arow = areg + (a + k - 1) * 16; // fast mode a+k-1
-  const f2_t *adup  = reinterpret_cast<const f2_t *>(areg + D * 16) + a * 16; // slow mode a
+  const float *srow = areg + a * 16;           // slow mode a
 
   for (int f = tid; f < F; f += PIPE_THREADS)
   {
@@ -409,49 +428,41 @@ __device__ __forceinline__ void pipe_pass_packed(const float *src, float *dst, c
     }
     float w[C];
     fast_mode<Q>(arow, V, w);
-    f2_t O[2 * Q];
+    // store 4 results q' (elements 4q' .. 4q'+3 of the fibre)
+    auto put4 = [&](int q, float o0, float o1, float o2, float o3) {
+      if constexpr (S == 1)
+        *reinterpret_cast<float4 *>(dst + fib_off<float, N, DST == DST_WORK>(sbd, 4 * q)) =
+            make_float4(o0, o1, o2, o3);
+      else
+      {
+        dst[fib_off<float, N, DST == DST_WORK>(sbd, (4 * q) * S)]     = o0;
+        dst[fib_off<float, N, DST == DST_WORK>(sbd, (4 * q + 1) * S)] = o1;
+        dst[fib_off<float, N, DST == DST_WORK>(sbd, (4 * q + 2) * S)] = o2;
+        dst[fib_off<float, N, DST == DST_WORK>(sbd, (4 * q + 3) * S)] = o3;
+      }
+    };
     if constexpr (k == 1)
-    {
-      O[0] = pk2(w[0], w[1]);
-      O[1] = pk2(w[2], w[3]);
-    }
+      put4(0, w[0], w[1], w[2], w[3]);
     else
     {
-      // slow mode a: out[4q' + t] = sum_j A_a(q', j) w[4j + t], t in pairs
+      // slow mode a: out[4q' + t] = sum_j A_a(q', j) w[4j + t], contracted
+      // in pairs {w[t], w[4+t]}, {w[8+t], w[12+t]}
       f2_t W[8];
 #pragma unroll
-      for (int j = 0; j < 4; j++)
+      for (int t = 0; t < 4; t++)
       {
-        W[2 * j]     = pk2(w[4 * j], w[4 * j + 1]);
-        W[2 * j + 1] = pk2(w[4 * j + 2], w[4 * j + 3]);
+        W[2 * t]     = pk2(w[t], w[4 + t]);
+        W[2 * t + 1] = pk2(w[8 + t], w[12 + t]);
       }
 #pragma unroll
       for (int qq = 0; qq < 4; qq++)
       {
-        const ulonglong2 D01 = *reinterpret_cast<const ulonglong2 *>(adup + 4 * qq);
-        const ulonglong2 D23 = *reinterpret_cast<const ulonglong2 *>(adup + 4 * qq + 2);
+        const ulonglong2 R = *reinterpret_cast<const ulonglong2 *>(srow + 4 * qq);
+        float o4[4];
 #pragma unroll
-        for (int tp = 0; tp < 2; tp++)
-          O[2 * qq + tp] =
-              fma2(D23.y, W[6 + tp], fma2(D23.x, W[4 + tp], fma2(D01.y, W[2 + tp], mul2(D01.x, W[tp]))));
-      }
-    }
-    if constexpr (S == 1)
-    {
-#pragma unroll
-      for (int q = 0; q < Q; q++)
-        *reinterpret_cast<ulonglong2 *>(dst + fib_off<float, N, DST == DST_WORK>(sbd, 4 * q)) =
-            make_ulonglong2(O[2 * q], O[2 * q + 1]);
-    }
-    else
-    {
-#pragma unroll
-      for (int c = 0; c < C; c += 2)
-      {
-        float x0, x1;
-        upk2(O[c / 2], x0, x1);
-        dst[fib_off<float, N, DST == DST_WORK>(sbd, c * S)]       = x0;
-        dst[fib_off<float, N, DST == DST_WORK>(sbd, (c + 1) * S)] = x1;
+        for (int t = 0; t < 4; t++)
+          o4[t] = hsum2(fma2(R.y, W[2 * t + 1], mul2(R.x, W[2 * t])));
+        put4(qq, o4[0], o4[1], o4[2], o4[3]);
       }
     }
   }
@@ -466,22 +477,6 @@ __device__ __forceinline__ void run_pass(const T *src, T *dst, const T *As, int 
   else
     pipe_pass<T, D, N, a, k, SRC_STAGE, DST>(src, dst, As, tid);
 }
-
-// Passes in order: group 0 (reads the stage), then the last group, then the
-// middle groups; the final pass writes the result into the stage for one
-// bulk reduce-add.
-template <typename T, int D, int N>
-struct PipePlan
-{
-  static constexpr int k      = GroupK<N>::k;
-  static constexpr int ngroup = (D + k - 1) / k;
-  static constexpr int last_a = (ngroup - 1) * k;
-  static constexpr int last_k = D - last_a;
-  // stride of the pass executed last (a middle group when ngroup >= 3)
-  static constexpr int final_a = ngroup >= 3 ? (ngroup - 2) * k : last_a;
-  static constexpr int final_k = ngroup >= 3 ? k : last_k;
-  static constexpr int final_S = cpow(N, D - final_a - final_k);
-};
 
 template <typename T, int D, int N, int gi>
 __device__ __forceinline__ void middle_passes(T *work, const T *As, int tid)
@@ -652,7 +647,10 @@ __global__ void __launch_bounds__(PIPE_THREADS, PipeOcc<T>::value)
     if constexpr (P::ngroup >= 3)
     {
       run_pass<T, D, N, P::last_a, P::last_k, false, DST_WORK>(work, work, As, tid);
-      __syncthreads();
+      if constexpr (P::WARP_LOCAL_TAIL)
+        __syncwarp(); // both passes keep to this warp's slabs
+      else
+        __syncthreads();
       middle_passes<T, D, N, 1>(work, As, tid);
       run_pass<T, D, N, P::final_a, P::final_k, false, DST_STAGE>(work, sx, As, tid);
     }
