@@ -279,6 +279,48 @@ int kron_measure_fp64_peak(double *tensor_tflops, double *cuda_core_tflops);
  * clear != 0 resets the word.  Returns -1 if it cannot be read. */
 int kron_device_status(int clear);
 
+/* ------------------------------------------------------------------------
+ * Autotuner (no reference counterpart).  For square shapes the library picks
+ * among kernel variants, each with one tuning parameter:
+ *   KRON_VARIANT_MMA8   FP64 tensor-core kernel for d = 3, n = 8
+ *   KRON_VARIANT_PIPE   TMA-pipelined passes (n = 3..5, 4-64 KB vectors)
+ *   KRON_VARIANT_SQ     on-chip square kernel; param = entries per thread
+ *                       block (0: as many as fit)
+ *   KRON_VARIANT_GEN    on-chip runtime-shape kernel
+ *   KRON_VARIANT_BIG    cluster two-phase kernel; param = cluster size
+ *                       (0: default)
+ *   KRON_VARIANT_LARGE  two-phase launches through the workspace W
+ * kron_autotune times every variant that runs (d, n, precision) on a
+ * synthetic batched problem of up to batchCount entries (capped at 1 GiB),
+ * records the fastest for that key and returns it (outputs may be NULL).
+ * It allocates and frees device memory and synchronises `stream`: call it
+ * at set-up, outside stream capture.  Every later call with that square
+ * shape and precision, in any layout, tries the recorded variant first and
+ * falls back to the built-in choice when the variant cannot run it.
+ * kron_tune_set records a choice by hand (variant 0 removes it),
+ * kron_tune_get reads it (variant 0: none), kron_tune_save / _load keep the
+ * table in a text file.  Precision codes: KRON_PREC_F64 (the drop-in and
+ * segmented calls), KRON_PREC_F32 (kronmult_batched_f32_async),
+ * KRON_PREC_SPLIT (kronmult_batched_split_async).
+ * ---------------------------------------------------------------------- */
+#define KRON_PREC_F64 0
+#define KRON_PREC_F32 1
+#define KRON_PREC_SPLIT 2
+#define KRON_VARIANT_MMA8 1
+#define KRON_VARIANT_PIPE 2
+#define KRON_VARIANT_SQ 3
+#define KRON_VARIANT_GEN 4
+#define KRON_VARIANT_BIG 5
+#define KRON_VARIANT_LARGE 6
+
+int kron_autotune(int d, int n, int precision, int batchCount, int *variant, int *param,
+                  double *best_us, kron_stream_t stream);
+int kron_tune_set(int d, int n, int precision, int variant, int param);
+int kron_tune_get(int d, int n, int precision, int *variant, int *param);
+void kron_tune_clear(void);
+int kron_tune_save(const char *path);
+int kron_tune_load(const char *path);
+
 #ifdef __cplusplus
 } /* extern "C" */
 

@@ -77,6 +77,12 @@ def _sig(lib):
     S["kron_version"] = []
     S["kron_measure_fp64_peak"] = [_vp, _vp]
     S["kron_device_status"] = [_i]
+    S["kron_autotune"] = [_i, _i, _i, _i, _vp, _vp, _vp, _vp]
+    S["kron_tune_set"] = [_i, _i, _i, _i, _i]
+    S["kron_tune_get"] = [_i, _i, _i, _vp, _vp]
+    S["kron_tune_clear"] = []
+    S["kron_tune_save"] = [C.c_char_p]
+    S["kron_tune_load"] = [C.c_char_p]
     for name, args in S.items():
         f = getattr(lib, name)
         f.argtypes = args
@@ -88,6 +94,7 @@ def _sig(lib):
     lib.kron_flops_c.restype = _d
     lib.kron_status_string.restype = C.c_char_p
     lib.kron_version.restype = C.c_char_p
+    lib.kron_tune_clear.restype = None
     return lib
 
 
@@ -190,6 +197,46 @@ def measure_fp64_peak():
     a, b = C.c_double(), C.c_double()
     _check(lib().kron_measure_fp64_peak(C.byref(a), C.byref(b)), "kron_measure_fp64_peak")
     return a.value, b.value
+
+
+# ---------------------------------------------------------------- autotuner
+PRECISIONS = {"f64": 0, "f32": 1, "split": 2}
+VARIANTS = {1: "mma8", 2: "pipe", 3: "sq", 4: "gen", 5: "big", 6: "large"}
+
+
+def autotune(d, n, precision="f64", batch=1024, stream=None):
+    """Time every kernel variant for square (d, n) at `precision` on a
+    synthetic batch and record the fastest; returns (variant, param, us)."""
+    v, q, t = C.c_int(), C.c_int(), C.c_double()
+    _check(lib().kron_autotune(d, n, PRECISIONS[precision], batch, C.byref(v), C.byref(q),
+                               C.byref(t), _stream(stream)), "kron_autotune")
+    return VARIANTS[v.value], q.value, t.value
+
+
+def tune_set(d, n, precision, variant, param=0):
+    """Record a variant by name ("sq", "big", ...; None removes the entry)."""
+    code = 0 if variant is None else {v: k for k, v in VARIANTS.items()}[variant]
+    _check(lib().kron_tune_set(d, n, PRECISIONS[precision], code, param), "kron_tune_set")
+
+
+def tune_get(d, n, precision="f64"):
+    """(variant name or None, param) recorded for (d, n, precision)."""
+    v, q = C.c_int(), C.c_int()
+    _check(lib().kron_tune_get(d, n, PRECISIONS[precision], C.byref(v), C.byref(q)),
+           "kron_tune_get")
+    return VARIANTS.get(v.value), q.value
+
+
+def tune_clear():
+    lib().kron_tune_clear()
+
+
+def tune_save(path):
+    _check(lib().kron_tune_save(os.fsencode(path)), "kron_tune_save")
+
+
+def tune_load(path):
+    _check(lib().kron_tune_load(os.fsencode(path)), "kron_tune_load")
 
 
 class Segments:

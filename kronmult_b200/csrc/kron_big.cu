@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
 }
 
 template <typename T, int D, int N, int Q, int C, int MINB>
-int launch_big_t(Params p, const Workspace &wsp, int prec, cudaStream_t stream)
+int launch_big_t(Params p, const Workspace &wsp, int prec, int cluster, cudaStream_t stream)
 {
   using S        = BigShape<T, D, N, Q, C>;
   const void *fn = reinterpret_cast<const void *>(&kron_big_kernel<T, D, N, Q, C, MINB>);
@@ -521,7 +521,9 @@ int launch_big_t(Params p, const Workspace &wsp, int prec, cudaStream_t stream)
 
   const long long work = p.eend - p.ebase;
   int cs               = 2;
-  if (const char *env = std::getenv("KRON_BIG_CLUSTER"))
+  if (cluster > 0)
+    cs = std::min(8, cluster);
+  else if (const char *env = std::getenv("KRON_BIG_CLUSTER"))
     cs = std::max(1, std::min(8, std::atoi(env)));
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
@@ -561,7 +563,7 @@ bool big_supported(const Params &p, int prec)
   return false;
 }
 
-int launch_big(Params p, const Workspace &ws, int prec, cudaStream_t stream)
+int launch_big(Params p, const Workspace &ws, int prec, int cluster, cudaStream_t stream)
 {
   if (p.eend <= p.ebase)
     return KRON_SUCCESS;
@@ -570,19 +572,19 @@ int launch_big(Params p, const Workspace &ws, int prec, cudaStream_t stream)
   if (prec == PREC_F32)
   {
     if (p.d == 6 && n == 7)
-      return launch_big_t<float, 6, 7, 3, 32, 2>(p, ws, prec, stream);
+      return launch_big_t<float, 6, 7, 3, 32, 2>(p, ws, prec, cluster, stream);
     if (p.d == 6 && n == 8)
-      return launch_big_t<float, 6, 8, 3, 16, 2>(p, ws, prec, stream);
+      return launch_big_t<float, 6, 8, 3, 16, 2>(p, ws, prec, cluster, stream);
     return KRON_ERROR_NOT_SUPPORTED;
   }
   if (p.d == 6 && n == 6)
-    return launch_big_t<double, 6, 6, 3, 16, 2>(p, ws, prec, stream);
+    return launch_big_t<double, 6, 6, 3, 16, 2>(p, ws, prec, cluster, stream);
   if (p.d == 6 && n == 7)
-    return launch_big_t<double, 6, 7, 3, 8, 2>(p, ws, prec, stream);
+    return launch_big_t<double, 6, 7, 3, 8, 2>(p, ws, prec, cluster, stream);
   if (p.d == 6 && n == 8)
-    return launch_big_t<double, 6, 8, 3, 16, 1>(p, ws, prec, stream);
+    return launch_big_t<double, 6, 8, 3, 16, 1>(p, ws, prec, cluster, stream);
   if (p.d == 5 && n == 8)
-    return launch_big_t<double, 5, 8, 2, 32, 1>(p, ws, prec, stream);
+    return launch_big_t<double, 5, 8, 2, 32, 1>(p, ws, prec, cluster, stream);
   return KRON_ERROR_NOT_SUPPORTED;
 }
 

@@ -287,6 +287,8 @@ static void setup_items(Params &p, const Workspace &ws)
   p.nitems = (p.eend - p.ebase + p.chunk - 1) / p.chunk;
 }
 
+void launch_setup(Params &p, const Workspace &ws) { setup_items(p, ws); }
+
 size_t large_workspace_elems(int d, const int *m, const int *n)
 {
   LargePlan lp;
@@ -453,6 +455,63 @@ bool fits_on_chip(int d, const int *m, const int *n, int precision, bool merge)
   return gen_whole_view(d, m, n, merge, precision == PREC_F32 ? 4 : 8, v);
 }
 
+int sq_entries_max(int prec, int d, int n, bool merge)
+{
+  if (n < 2 || n > 8)
+    return 0;
+  SqKernelInfo ki = pick_sq(prec, d, n, merge);
+  if (!ki.fn && merge)
+    ki = pick_sq(prec, d, n, false); // atomic without run merging
+  if (!ki.fn || ki.group_bytes > (size_t)device_info().max_smem_optin)
+    return 0;
+  return std::max(1, std::min(256 / ki.GS, (int)(device_info().max_smem_optin / ki.group_bytes)));
+}
+
+int launch_variant(Params p, int prec, const Workspace &ws, int variant, int param,
+                   cudaStream_t stream)
+{
+  const bool merge = (p.accum == ACC_ATOMIC || p.accum == ACC_SEGMENTED);
+  const int esize  = (prec == PREC_F32) ? 4 : 8;
+  switch (variant)
+  {
+  case VAR_MMA8:
+    return mma8_supported(p, prec) ? launch_mma8(p, stream) : KRON_ERROR_NOT_SUPPORTED;
+  case VAR_PIPE:
+    return pipe_supported(p, prec) ? launch_pipe(p, prec, stream) : KRON_ERROR_NOT_SUPPORTED;
+  case VAR_SQ: {
+    if (!is_square(p))
+      return KRON_ERROR_NOT_SUPPORTED;
+    const int ngmax = sq_entries_max(prec, p.d, p.n[0], merge);
+    if (ngmax < 1)
+      return KRON_ERROR_NOT_SUPPORTED;
+    SqKernelInfo ki = pick_sq(prec, p.d, p.n[0], merge);
+    if (!ki.fn)
+      ki = pick_sq(prec, p.d, p.n[0], false);
+    const int ng   = param > 0 ? std::min(param, ngmax) : ngmax;
+    const int block = ng * ki.GS;
+    size_t smem     = (size_t)ng * ki.group_bytes;
+    void *args[]    = {&p};
+    return launch_blocks(ki.fn, p.nitems, ng, block, smem, args, stream);
+  }
+  case VAR_GEN: {
+    GenView v;
+    if (gen_whole_view(p.d, p.m, p.n, merge, esize, v))
+      return launch_gen_prec(prec, p, v, stream);
+    if (merge && gen_whole_view(p.d, p.m, p.n, false, esize, v))
+      return launch_gen_prec(prec, p, v, stream);
+    return KRON_ERROR_NOT_SUPPORTED;
+  }
+  case VAR_BIG:
+    return big_supported(p, prec) ? launch_big(p, ws, prec, param, stream)
+                                  : KRON_ERROR_NOT_SUPPORTED;
+  case VAR_LARGE:
+    if (prec == PREC_F32)
+      return launch_large_t<float>(prec, p, ws, stream);
+    return launch_large_t<double>(prec, p, ws, stream);
+  default: return KRON_ERROR_NOT_SUPPORTED;
+  }
+}
+
 int launch_kron(Params p, int prec, const Workspace &ws, cudaStream_t stream)
 {
   if (p.batch <= 0 || p.eend <= p.ebase)
@@ -460,49 +519,30 @@ int launch_kron(Params p, int prec, const Workspace &ws, cudaStream_t stream)
   setup_items(p, ws);
   if (p.nitems <= 0)
     return KRON_SUCCESS;
-  const bool merge = (p.accum == ACC_ATOMIC || p.accum == ACC_SEGMENTED);
-  const int esize  = (prec == PREC_F32) ? 4 : 8;
 
-  if (mma8_supported(p, prec) && !std::getenv("KRON_DISABLE_MMA8"))
-    return launch_mma8(p, stream);
-  if (pipe_supported(p, prec) && !std::getenv("KRON_DISABLE_PIPE"))
+  // a variant recorded for this (d, n, precision) goes first; one that
+  // cannot run this call (layout, accumulation mode, or a workspace the
+  // caller did not pass) leaves it to the built-in order
+  int tv = 0, tp = 0;
+  if (is_square(p) && tune_lookup(p.d, p.n[0], prec, tv, tp))
   {
-    int rc = launch_pipe(p, prec, stream);
+    const int rc = launch_variant(p, prec, ws, tv, tp, stream);
+    if (rc != KRON_ERROR_NOT_SUPPORTED && rc != KRON_ERROR_WORKSPACE)
+      return rc;
+  }
+  // default order: the specialised kernels, then the general ones
+  static const int order[] = {VAR_MMA8, VAR_PIPE, VAR_SQ, VAR_GEN, VAR_BIG, VAR_LARGE};
+  for (int v : order)
+  {
+    if ((v == VAR_MMA8 && std::getenv("KRON_DISABLE_MMA8")) ||
+        (v == VAR_PIPE && std::getenv("KRON_DISABLE_PIPE")) ||
+        (v == VAR_BIG && std::getenv("KRON_DISABLE_BIG")))
+      continue;
+    const int rc = launch_variant(p, prec, ws, v, 0, stream);
     if (rc != KRON_ERROR_NOT_SUPPORTED)
       return rc;
   }
-
-  if (is_square(p) && p.n[0] >= 2 && p.n[0] <= 8)
-  {
-    SqKernelInfo ki = pick_sq(prec, p.d, p.n[0], merge);
-    if (!ki.fn && merge)
-      ki = pick_sq(prec, p.d, p.n[0], false); // atomic without run merging
-    if (ki.fn && ki.group_bytes <= (size_t)device_info().max_smem_optin)
-    {
-      int ng      = std::max(1, std::min(256 / ki.GS,
-                                         (int)(device_info().max_smem_optin / ki.group_bytes)));
-      int block   = ng * ki.GS;
-      size_t smem = (size_t)ng * ki.group_bytes;
-      void *args[] = {&p};
-      return launch_blocks(ki.fn, p.nitems, ng, block, smem, args, stream);
-    }
-  }
-
-  GenView v;
-  if (gen_whole_view(p.d, p.m, p.n, merge, esize, v))
-    return launch_gen_prec(prec, p, v, stream);
-  if (merge && gen_whole_view(p.d, p.m, p.n, false, esize, v))
-    return launch_gen_prec(prec, p, v, stream);
-
-  if (big_supported(p, prec) && !std::getenv("KRON_DISABLE_BIG"))
-  {
-    int rc = launch_big(p, ws, prec, stream);
-    if (rc != KRON_ERROR_NOT_SUPPORTED)
-      return rc;
-  }
-  if (prec == PREC_F32)
-    return launch_large_t<float>(prec, p, ws, stream);
-  return launch_large_t<double>(prec, p, ws, stream);
+  return KRON_ERROR_NOT_SUPPORTED;
 }
 
 } // namespace kron

@@ -34,8 +34,33 @@ int launch_mma8(Params p, cudaStream_t stream);
 bool pipe_supported(const Params &p, int prec);
 int launch_pipe(Params p, int prec, cudaStream_t stream);
 
-// Cluster two-phase kernel for vectors beyond shared memory (kron_big.cu).
+// Cluster two-phase kernel for vectors beyond shared memory (kron_big.cu);
+// cluster <= 0 picks the default cluster size.
 bool big_supported(const Params &p, int prec);
-int launch_big(Params p, const Workspace &ws, int prec, cudaStream_t stream);
+int launch_big(Params p, const Workspace &ws, int prec, int cluster, cudaStream_t stream);
+
+// Kernel variants the launcher chooses among (values of KRON_VARIANT_* in
+// kronmult.h).
+enum Variant : int
+{
+  VAR_NONE  = 0,
+  VAR_MMA8  = 1, // FP64 tensor-core d = 3, n = 8 (param unused)
+  VAR_PIPE  = 2, // TMA-pipelined register-blocked passes (param unused)
+  VAR_SQ    = 3, // square on-chip kernel; param = entries per block (0: most that fit)
+  VAR_GEN   = 4, // runtime-shape on-chip kernel (param unused)
+  VAR_BIG   = 5, // cluster two-phase kernel; param = cluster size (0: default)
+  VAR_LARGE = 6, // two-phase launches through the workspace (param unused)
+};
+
+// Work items of a launch (launch_kron does this before any variant).
+void launch_setup(Params &p, const Workspace &ws);
+// Launch one variant; KRON_ERROR_NOT_SUPPORTED when it cannot run p.
+int launch_variant(Params p, int prec, const Workspace &ws, int variant, int param,
+                   cudaStream_t stream);
+// Most entries per block of the square on-chip kernel for (d, n), 0 when it
+// does not apply.
+int sq_entries_max(int prec, int d, int n, bool merge);
+// Variant recorded for (d, n, prec) by the autotuner or the caller.
+bool tune_lookup(int d, int n, int prec, int &variant, int &param);
 
 } // namespace kron
