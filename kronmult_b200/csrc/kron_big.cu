@@ -8,9 +8,9 @@
 //            FP64 tensor-core routine of kron_mma8_core.cuh), result -> W;
 //   barrier.cluster (hardware, no spinning) -- W is complete;
 //   phase 2: every column tile (LH rows x C columns of W, C contiguous
-//            doubles per row) gets the head modes in shared memory and is
-//            added into y (batched loads before stores, or red.global.add
-//            for aliasing outputs).
+//            doubles per row), fetched by cp.async one tile ahead, gets the
+//            head modes in shared memory and is added into y with
+//            red.global.add (one rounding, as y += r; no load round trip).
 // This is the recursive algorithm's two-level split (kronmultv_recur.hpp:
 // 117-145 applies A_1 on X viewed as (n2..nd) x n1, then recurses), with
 // the intermediate W kept L2-resident: only one entry per cluster is in
@@ -103,9 +103,10 @@ struct BigShape
   static constexpr int TBUF  = ((MMA2 ? C * PITCH : LH * C) + 15) / 16 * 16;
   static constexpr size_t OFF_A    = 0;
   static constexpr size_t OFF_R    = OFF_A + (size_t)ASZ * sizeof(T);           // 2 round buffers
-  // the tensor-core phases use one round and one tile buffer, the others two
+  // the tensor-core phase 1 uses one round buffer, the others two; phase 2
+  // double-buffers its tiles
   static constexpr size_t OFF_TILE = OFF_R + (MMA ? 1 : 2) * (size_t)RBUF * sizeof(T);
-  static constexpr size_t SMEM     = OFF_TILE + (MMA2 ? 1 : 2) * (size_t)TBUF * sizeof(T);
+  static constexpr size_t SMEM     = OFF_TILE + 2 * (size_t)TBUF * sizeof(T);
 };
 
 template <typename T>
@@ -248,10 +249,10 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
                   reinterpret_cast<const double *>(en.A[Q + 1]), en.ld[Q + 1],
                   reinterpret_cast<const double *>(en.A[Q + 2]), en.ld[Q + 2], g, t);
       const bool al16 = ((reinterpret_cast<uintptr_t>(en.x) & 15) == 0);
-      for (int h = hb + warp; h < he; h += BIG_WARPS)
-      {
+      // this lane's 16 elements of head row h (the next row is loaded while
+      // the current one is on the tensor cores)
+      auto load_row = [&](int h, double (&v)[8][2]) {
         const double *xb = reinterpret_cast<const double *>(en.x) + (long long)h * LT;
-        double v[8][2], acc[8][2];
 #pragma unroll
         for (int q = 0; q < 8; q++)
         {
@@ -267,8 +268,23 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
             v[q][0] = __ldg(src);
             v[q][1] = __ldg(src + 1);
           }
+        }
+      };
+      double vn[8][2];
+      if (hb + warp < he)
+        load_row(hb + warp, vn);
+      for (int h = hb + warp; h < he; h += BIG_WARPS)
+      {
+        double v[8][2], acc[8][2];
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+        {
+          v[q][0] = vn[q][0];
+          v[q][1] = vn[q][1];
           acc[q][0] = acc[q][1] = 0.0;
         }
+        if (h + BIG_WARPS < he)
+          load_row(h + BIG_WARPS, vn);
         kron8x3_tile(v, acc, f, blk, g, t);
         double *wb = reinterpret_cast<double *>(w) + (long long)h * LT;
 #pragma unroll
@@ -321,7 +337,7 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
     {
       constexpr int PITCH = S::PITCH;
       const int g = lane >> 2, t = lane & 3;
-      double *tile = reinterpret_cast<double *>(tbuf0);
+      double *tiles = reinterpret_cast<double *>(tbuf0);
       double *xs   = reinterpret_cast<double *>(rbuf0) + warp * 512; // transpose scratch
       AFrag8 f;
       load_afrag8(f, reinterpret_cast<const double *>(en.A[0]), en.ld[0],
@@ -329,32 +345,34 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
                   reinterpret_cast<const double *>(en.A[2]), en.ld[2], g, t);
       const double *wd = reinterpret_cast<const double *>(w);
       double *yd       = reinterpret_cast<double *>(en.y);
+      // W rows -> transposed tile (column c contiguous) by cp.async, one
+      // tile ahead of the one being computed
+      auto issue_gather = [&](int tt, double *tile) {
+        const int c0 = tt * C, cc = min(C, LT - c0);
+        for (int q = tid; q < LH * C; q += BIG_THREADS)
+        {
+          const int h = q / C, c = q - (q / C) * C;
+          if (c < cc)
+            cp_async_elem(tile + c * PITCH + h, wd + (long long)h * LT + c0 + c);
+          else
+            tile[c * PITCH + h] = 0.0;
+        }
+        cp_commit();
+      };
+      int cur = 0;
+      if (tb < te)
+        issue_gather(tb, tiles);
       for (int tt = tb; tt < te; ++tt)
       {
         const int c0 = tt * C, cc = min(C, LT - c0);
-        // W rows -> transposed tile (column c contiguous), loads batched
-        constexpr int B = 8;
-        for (int q0 = tid; q0 < LH * C; q0 += BIG_THREADS * B)
+        double *tile = tiles + cur * S::TBUF;
+        if (tt + 1 < te)
         {
-          double vals[B];
-#pragma unroll
-          for (int b = 0; b < B; b++)
-          {
-            const int q = q0 + b * BIG_THREADS;
-            const int h = q / C, c = q - (q / C) * C;
-            vals[b] = (q < LH * C && c < cc) ? wd[(long long)h * LT + c0 + c] : 0.0;
-          }
-#pragma unroll
-          for (int b = 0; b < B; b++)
-          {
-            const int q = q0 + b * BIG_THREADS;
-            if (q < LH * C)
-            {
-              const int h = q / C, c = q - (q / C) * C;
-              tile[c * PITCH + h] = vals[b];
-            }
-          }
+          issue_gather(tt + 1, tiles + (cur ^ 1) * S::TBUF);
+          cp_wait<1>();
         }
+        else
+          cp_wait<0>();
         __syncthreads();
         // each warp: kron(A_1, A_2, A_3) on whole columns
         for (int c = warp; c < cc; c += BIG_WARPS)
@@ -378,37 +396,19 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
                 make_double2(acc[q][0], acc[q][1]);
         }
         __syncthreads();
-        // tile rows into y, loads batched ahead of stores
-        for (int q0 = tid; q0 < LH * C; q0 += BIG_THREADS * B)
+        // tile rows into y by red.global.add (fire and forget; each output
+        // element has one writer in this launch unless outputs alias)
+        for (int q = tid; q < LH * C; q += BIG_THREADS)
         {
-          double old[B];
-          if (p.accum != ACC_ATOMIC)
-#pragma unroll
-            for (int b = 0; b < B; b++)
-            {
-              const int q = q0 + b * BIG_THREADS;
-              const int i = q / C, c = q - (q / C) * C;
-              if (q < LH * C && c < cc)
-                old[b] = yd[(long long)i * LT + c0 + c];
-            }
-#pragma unroll
-          for (int b = 0; b < B; b++)
+          const int i = q / C, c = q - (q / C) * C;
+          if (c < cc)
           {
-            const int q = q0 + b * BIG_THREADS;
-            const int i = q / C, c = q - (q / C) * C;
-            if (q < LH * C && c < cc)
-            {
-              double *dst = yd + (long long)i * LT + c0 + c;
-              const int pos  = ((i >> 3) & 7) * 64 + (i & 7) * 8 + (i >> 6);
-              const double r = tile[c * PITCH + pos];
-              if (p.accum == ACC_ATOMIC)
-                red_add(dst, r);
-              else
-                *dst = old[b] + r;
-            }
+            const int pos = ((i >> 3) & 7) * 64 + (i & 7) * 8 + (i >> 6);
+            red_add(yd + (long long)i * LT + c0 + c, tile[c * PITCH + pos]);
           }
         }
         __syncthreads();
+        cur ^= 1;
       }
     }
     else
@@ -441,33 +441,12 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
         __syncthreads();
         tile_head_passes<T, N, Q, C, 0>(tile, As, tid);
         const int c0 = tt * C, cc = min(C, LT - c0);
-        constexpr int B = 4;
-        for (int q0 = tid; q0 < LH * C; q0 += BIG_THREADS * B)
+        // tile rows into y by red.global.add (fire and forget)
+        for (int q = tid; q < LH * C; q += BIG_THREADS)
         {
-          T old[B];
-          if (p.accum != ACC_ATOMIC)
-#pragma unroll
-            for (int b = 0; b < B; b++)
-            {
-              const int q = q0 + b * BIG_THREADS;
-              const int i = q / C, c = q - (q / C) * C;
-              if (q < LH * C && c < cc)
-                old[b] = en.y[(long long)i * LT + c0 + c];
-            }
-#pragma unroll
-          for (int b = 0; b < B; b++)
-          {
-            const int q = q0 + b * BIG_THREADS;
-            const int i = q / C, c = q - (q / C) * C;
-            if (q < LH * C && c < cc)
-            {
-              T *dst = en.y + (long long)i * LT + c0 + c;
-              if (p.accum == ACC_ATOMIC)
-                red_add(dst, tile[q]);
-              else
-                *dst = old[b] + tile[q];
-            }
-          }
+          const int i = q / C, c = q - (q / C) * C;
+          if (c < cc)
+            red_add(en.y + (long long)i * LT + c0 + c, tile[q]);
         }
         __syncthreads();
         cur ^= 1;
