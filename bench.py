@@ -596,8 +596,8 @@ def dist_setup():
 # ---------------------------------------------------------------- reference arm
 def run_reference(args, world, rank):
     """The reference's own CPU (OpenMP) implementation of the same workload,
-    on the host cores: oracle/_ref (compiled from the reference sources) when
-    present, else the oracle's C port."""
+    on the host cores: oracle/_ref, compiled from the reference sources by
+    oracle/Makefile.  Without that build it prints the `unavailable` line."""
     if rank != 0:
         return
     import oracle
