@@ -396,6 +396,66 @@ struct GenView
   int merge;
 };
 
+// One mode on fibres of compile-time length: input sizes NQ, output MQ,
+// fibre f = (o, r) reads cur[(o NQ + j) in32 + r], writes
+// nxt[(o MQ + i) in32 + r].  Small factors live in registers, larger ones
+// are read from shared memory (broadcast) where they are used.
+template <typename T, int NQ, int MQ>
+__device__ __forceinline__ void gen_mode_fibres(const T *cur, T *nxt, const T *Aq, int in32,
+                                                int nfib, int t, int GS)
+{
+  constexpr bool AREG = NQ * MQ <= 16;
+  T a[AREG ? MQ : 1][AREG ? NQ : 1];
+  if constexpr (AREG)
+  {
+#pragma unroll
+    for (int i = 0; i < MQ; i++)
+#pragma unroll
+      for (int j = 0; j < NQ; j++)
+        a[i][j] = Aq[i + j * MQ];
+  }
+  for (int f = t; f < nfib; f += GS)
+  {
+    const int o = f / in32, r = f - (f / in32) * in32;
+    const T *src = cur + (o * NQ) * in32 + r;
+    T *dst       = nxt + (o * MQ) * in32 + r;
+    T x[NQ];
+#pragma unroll
+    for (int j = 0; j < NQ; j++)
+      x[j] = src[j * in32];
+#pragma unroll
+    for (int i = 0; i < MQ; i++)
+    {
+      T z = T(0);
+#pragma unroll
+      for (int j = 0; j < NQ; j++)
+        z = fma(AREG ? a[i][j] : Aq[i + j * MQ], x[j], z);
+      dst[i * in32] = z;
+    }
+  }
+}
+
+// dispatch (nq, mq) in 1..8 to the compile-time fibre pass; false when
+// out of range
+template <typename T>
+__device__ __forceinline__ bool gen_mode_sized(int nq, int mq, const T *cur, T *nxt, const T *Aq,
+                                               int in32, int nfib, int t, int GS)
+{
+#define KRON_GM(NQ_, MQ_)                                                                       \
+  case NQ_ * 16 + MQ_: gen_mode_fibres<T, NQ_, MQ_>(cur, nxt, Aq, in32, nfib, t, GS); return true;
+#define KRON_GM_ROW(NQ_)                                                                        \
+  KRON_GM(NQ_, 1) KRON_GM(NQ_, 2) KRON_GM(NQ_, 3) KRON_GM(NQ_, 4) KRON_GM(NQ_, 5)              \
+  KRON_GM(NQ_, 6) KRON_GM(NQ_, 7) KRON_GM(NQ_, 8)
+  switch (nq * 16 + mq)
+  {
+    KRON_GM_ROW(1) KRON_GM_ROW(2) KRON_GM_ROW(3) KRON_GM_ROW(4)
+    KRON_GM_ROW(5) KRON_GM_ROW(6) KRON_GM_ROW(7) KRON_GM_ROW(8)
+  default: return false;
+  }
+#undef KRON_GM_ROW
+#undef KRON_GM
+}
+
 template <typename T, int PREC>
 __device__ void gen_apply_modes(const GenView &v, T *&cur, T *&nxt, const T *As, int C, int t,
                                 int GS, int g)
@@ -424,7 +484,12 @@ __device__ void gen_apply_modes(const GenView &v, T *&cur, T *&nxt, const T *As,
       inner *= dims[u];
     const T *Aq         = As + aoff[q]; // Aq[i + j*mq]
     const long long tot = outer * mq * inner;
-    if (PREC != PREC_SPLIT && nq <= 8 && tot < (1LL << 31))
+    if (PREC != PREC_SPLIT && nq <= 8 && mq <= 8 && tot < (1LL << 31) &&
+        gen_mode_sized<T>(nq, mq, cur, nxt, Aq, (int)inner, (int)(outer * inner), t, GS))
+    {
+      // fibre per thread with compile-time sizes (done above)
+    }
+    else if (PREC != PREC_SPLIT && nq <= 8 && tot < (1LL << 31))
     {
       // fibre per thread: its nq inputs are read once, all mq outputs formed
       // from them (A broadcast from shared memory); 32-bit index math

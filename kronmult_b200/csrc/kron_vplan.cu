@@ -8,14 +8,21 @@
 //     (kronm.hpp:39-89), and the largest intermediate of that order;
 //   - a class by that size: "warp" (<= 512 elements: one warp per entry,
 //     eight entries per block), "block" (fits the block's shared memory
-//     twice: one block per entry), "huge" (beyond: per-block two-phase
-//     split through the workspace, sizes chosen like the uniform path);
-//   - within each class, entries sorted by flops, largest first.
-// kron_vplan_execute_async then runs two persistent launches (huge; block
-// then warp class) that take entries from device work counters, so the
-// largest entries start first and the small ones fill the tail.  On a
-// non-default stream the counter reset and both launches are captured once
-// into a CUDA graph and replayed while the operand arrays stay the same.
+//     twice: one block per entry), "huge" (beyond: a two-phase split, head
+//     modes [0, q) and tail modes [q, d), sizes chosen like the uniform
+//     path);
+//   - every huge entry is cut into work items: row items (phase 1: the tail
+//     modes on a range of head rows, written to the entry's own region of
+//     the workspace) and tile items (phase 2: the head modes on a range of
+//     column tiles of that region, added into y), so all SMs share the
+//     largest entries;
+//   - within each list, items sorted by cost, largest first.
+// kron_vplan_execute_async runs one persistent kernel twice: stage 0 takes
+// huge row items, then block-class entries, then warp-class entries from
+// device work counters; stage 1 (after the launch boundary, the only
+// dependency) takes the tile items.  On a non-default stream the counter
+// reset and both launches are captured once into a CUDA graph and replayed
+// while the operand arrays stay the same.
 #include <algorithm>
 #include <cstring>
 #include <new>
@@ -35,6 +42,7 @@ constexpr int CLS_WARP    = 0, CLS_BLOCK = 1, CLS_HUGE = 2;
 
 struct VDesc
 {
+  long long woff;       // huge: element offset of the entry's workspace region
   int k;                // entry index (operands at pA[6k + l], pX[k], pY[k])
   unsigned char d, fwd, q, C;  // order; huge: head modes q, tile columns C
   unsigned char m[6], n[6];
@@ -45,16 +53,25 @@ struct VDesc
                                     // elements / 16 (rounded up)
 };
 
+// a range [lo, hi) of head rows (phase 1) or column tiles (phase 2) of the
+// huge entry desc[d]
+struct VItem
+{
+  int d, lo, hi, pad;
+};
+
 struct VParams
 {
-  const VDesc *desc;
-  int nhuge, nblock, nwarp;   // descriptors: [huge | block | warp]
-  int *counters;              // 3 work counters (zeroed before every execution)
+  const VDesc *desc;          // [huge | block | warp]
+  const VItem *items;         // [row items | tile items]
+  int nhuge, nblock, nwarp;
+  int nrow, ntile;
+  int stage;                  // 0: row items, block and warp classes; 1: tile items
+  int *counters;              // work counters (zeroed before every execution)
   const double *const *pA;
   const double *const *pX;
   double *const *pY;
-  double *ws;                 // huge class: per-block slot
-  long long slot_elems;
+  double *ws;                 // huge class: per-entry regions
   int block_elems;            // shared elements per block in block mode
 };
 
@@ -134,31 +151,121 @@ __device__ __forceinline__ void vp_operands(const VParams &vp, const VDesc &e, c
   y = vp.pY[e.k];
 }
 
-// block class, then warp class, from two work counters
+// Sizes of a huge entry's split: head inputs Nhead, tail inputs / outputs
+// Ntail, Mtail (phase 1 maps each head row of Ntail elements to Mtail).
+struct HugeDims
+{
+  int Nhead, Ntail, Mtail;
+};
+
+__device__ __forceinline__ HugeDims huge_dims(const VDesc &e)
+{
+  HugeDims h{1, 1, 1};
+  for (int l = 0; l < e.q; l++)
+    h.Nhead *= e.n[l];
+  for (int l = e.q; l < e.d; l++)
+  {
+    h.Ntail *= e.n[l];
+    h.Mtail *= e.m[l];
+  }
+  return h;
+}
+
+// next work item of a list for the whole block
+__device__ __forceinline__ int block_take(int *counter, int *s_idx, int tid)
+{
+  if (tid == 0)
+    *s_idx = atomicAdd(counter, 1);
+  __syncthreads();
+  const int idx = *s_idx;
+  __syncthreads();
+  return idx;
+}
+
+// Stage 0: huge row items, block class, warp class.  Stage 1: huge tile
+// items.  Counters: [0] row items, [1] block class, [2] warp class,
+// [3] tile items.
 __global__ void __launch_bounds__(VP_THREADS, 1) kron_vplan_kernel(const __grid_constant__ VParams vp)
 {
   extern __shared__ __align__(16) double smem[];
   __shared__ int s_idx;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const double *A[6];
+  int ld[6];
+  const double *x;
+  double *y;
+
+  if (vp.stage == 1)
+  {
+    // ---- phase 2 of huge entries: head modes on column tiles -> y
+    while (true)
+    {
+      const int idx = block_take(&vp.counters[3], &s_idx, tid);
+      if (idx >= vp.ntile)
+        break;
+      const VItem it = vp.items[vp.nrow + idx];
+      const VDesc e  = vp.desc[it.d];
+      vp_operands(vp, e, A, ld, x, y);
+      const HugeDims hd = huge_dims(e);
+      const double *wr  = vp.ws + e.woff;
+      GenView v2;
+      vp_view(v2, e, 0, e.q);
+      v2.forward = e.fwd2;
+      v2.C       = e.C;
+      v2.in_row = v2.out_row = hd.Mtail;
+      const int mi2 = e.mi2;
+      for (int t = it.lo; t < it.hi; t++)
+      {
+        const int c0  = t * e.C;
+        v2.total_cols = min((int)e.C, hd.Mtail - c0);
+        vp_group_entry(v2, true, wr + c0, y + c0, ACC_ATOMIC, smem, smem + mi2, smem + 2 * mi2,
+                       A, ld, tid, VP_THREADS, 0);
+      }
+    }
+    return;
+  }
+
+  // ---- phase 1 of huge entries: tail modes on head rows -> the entry's region
+  while (true)
+  {
+    const int idx = block_take(&vp.counters[0], &s_idx, tid);
+    if (idx >= vp.nrow)
+      break;
+    const VItem it = vp.items[idx];
+    const VDesc e  = vp.desc[it.d];
+    vp_operands(vp, e, A, ld, x, y);
+    const HugeDims hd = huge_dims(e);
+    double *wr        = vp.ws + e.woff;
+    GenView v1;
+    vp_view(v1, e, e.q, e.d - e.q);
+    v1.forward    = e.fwd1;
+    const int mi1 = e.mi;
+    if (e.pad[0])
+    {
+      // one head row per warp (the plan checked that eight slices fit)
+      const int slice = (2 * mi1 + e.pad[1] * 16 + 1) & ~1;
+      double *b0      = smem + warp * slice;
+      for (int h = it.lo + warp; h < it.hi; h += VP_WARPS)
+        vp_group_entry(v1, false, x + (long long)h * hd.Ntail, wr + (long long)h * hd.Mtail,
+                       ACC_STORE, b0, b0 + mi1, b0 + 2 * mi1, A, ld, lane, 32, warp);
+    }
+    else
+      for (int h = it.lo; h < it.hi; h++)
+        vp_group_entry(v1, false, x + (long long)h * hd.Ntail, wr + (long long)h * hd.Mtail,
+                       ACC_STORE, smem, smem + mi1, smem + 2 * mi1, A, ld, tid, VP_THREADS, 0);
+    __syncthreads();
+  }
 
   // ---- block class: the whole block per entry
   const VDesc *blk = vp.desc + vp.nhuge;
   while (true)
   {
-    if (tid == 0)
-      s_idx = atomicAdd(&vp.counters[1], 1);
-    __syncthreads();
-    const int idx = s_idx;
-    __syncthreads();
+    const int idx = block_take(&vp.counters[1], &s_idx, tid);
     if (idx >= vp.nblock)
       break;
     const VDesc e = blk[idx];
     GenView v;
     vp_view(v, e, 0, e.d);
-    const double *A[6];
-    int ld[6];
-    const double *x;
-    double *y;
     vp_operands(vp, e, A, ld, x, y);
     const int mi = (e.mi + 1) & ~1;
     vp_group_entry(v, false, x, y, ACC_ATOMIC, smem, smem + mi, smem + 2 * mi, A, ld, tid,
@@ -166,7 +273,6 @@ __global__ void __launch_bounds__(VP_THREADS, 1) kron_vplan_kernel(const __grid_
   }
 
   // ---- warp class: one warp per entry
-  const int warp = tid >> 5, lane = tid & 31;
   const int slice = vp.block_elems / VP_WARPS;
   double *b0      = smem + warp * slice;
   const VDesc *wd = vp.desc + vp.nhuge + vp.nblock;
@@ -181,84 +287,9 @@ __global__ void __launch_bounds__(VP_THREADS, 1) kron_vplan_kernel(const __grid_
     const VDesc e = wd[idx];
     GenView v;
     vp_view(v, e, 0, e.d);
-    const double *A[6];
-    int ld[6];
-    const double *x;
-    double *y;
     vp_operands(vp, e, A, ld, x, y);
     vp_group_entry(v, false, x, y, ACC_ATOMIC, b0, b0 + WARP_MAX, b0 + 2 * WARP_MAX, A, ld, lane,
                    32, warp);
-  }
-}
-
-// huge class: per block, phase 1 (tail modes on each head block -> slot),
-// phase 2 (head modes on column tiles of the slot -> y)
-__global__ void __launch_bounds__(VP_THREADS, 1)
-    kron_vplan_huge_kernel(const __grid_constant__ VParams vp)
-{
-  extern __shared__ __align__(16) double smem[];
-  __shared__ int s_idx;
-  const int tid = threadIdx.x;
-  double *slot  = vp.ws + (long long)blockIdx.x * vp.slot_elems;
-  while (true)
-  {
-    if (tid == 0)
-      s_idx = atomicAdd(&vp.counters[0], 1);
-    __syncthreads();
-    const int idx = s_idx;
-    __syncthreads();
-    if (idx >= vp.nhuge)
-      break;
-    const VDesc e = vp.desc[idx];
-    const int d = e.d, q = e.q, C = e.C;
-    const double *A[6];
-    int ld[6];
-    const double *x;
-    double *y;
-    vp_operands(vp, e, A, ld, x, y);
-    int Nhead = 1, Ntail = 1, Mtail = 1;
-    for (int l = 0; l < q; l++)
-      Nhead *= e.n[l];
-    for (int l = q; l < d; l++)
-    {
-      Ntail *= e.n[l];
-      Mtail *= e.m[l];
-    }
-    // phase 1 (order and buffer size from the plan)
-    GenView v1;
-    vp_view(v1, e, q, d - q);
-    v1.forward    = e.fwd1;
-    const int mi1 = e.mi;
-    if (e.pad[0])
-    {
-      // one head block per warp, eight at a time (plan checked the slices fit)
-      const int warp = tid >> 5, lane = tid & 31;
-      const int slice = (2 * mi1 + e.pad[1] * 16 + 1) & ~1;
-      double *b0      = smem + warp * slice;
-      for (int h = warp; h < Nhead; h += VP_WARPS)
-        vp_group_entry(v1, false, x + (long long)h * Ntail, slot + (long long)h * Mtail,
-                       ACC_STORE, b0, b0 + mi1, b0 + 2 * mi1, A, ld, lane, 32, warp);
-    }
-    else
-      for (int h = 0; h < Nhead; h++)
-        vp_group_entry(v1, false, x + (long long)h * Ntail, slot + (long long)h * Mtail,
-                       ACC_STORE, smem, smem + mi1, smem + 2 * mi1, A, ld, tid, VP_THREADS, 0);
-    __threadfence_block();
-    __syncthreads();
-    // phase 2
-    GenView v2;
-    vp_view(v2, e, 0, q);
-    v2.forward    = e.fwd2;
-    v2.C          = C;
-    v2.in_row = v2.out_row = Mtail;
-    const int mi2 = e.mi2;
-    for (int c0 = 0; c0 < Mtail; c0 += C)
-    {
-      v2.total_cols = min(C, Mtail - c0);
-      vp_group_entry(v2, true, slot + c0, y + c0, ACC_ATOMIC, smem, smem + mi2, smem + 2 * mi2, A,
-                     ld, tid, VP_THREADS, 0);
-    }
-    __syncthreads();
   }
 }
 
@@ -268,11 +299,11 @@ struct kron_vplan_st
 {
   int batch;
   int nhuge, nblock, nwarp;
+  int nrow, ntile;
   VDesc *d_desc;
+  VItem *d_items;
   int *d_counters;
   double flops;
-  long long slot_elems;
-  int huge_grid;
   size_t ws_bytes;
   size_t smem_main, smem_huge;
   int block_elems;
@@ -294,7 +325,6 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
   std::vector<VDesc> cls[3];
   std::vector<double> cost[3];
   double total_flops   = 0.0;
-  long long max_slot   = 0;
   size_t smem_huge     = 0;
   for (int k = 0; k < batchCount; k++)
   {
@@ -341,7 +371,6 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
       e.fwd1 = (unsigned char)lp.v1.forward;
       e.fwd2 = (unsigned char)lp.v2.forward;
       e.mi2  = lp.v2.max_inter; // rows x C, rounded
-      max_slot = std::max(max_slot, lp.slot_elems);
       size_t need = (size_t)std::max(lp.v1.group_elems, lp.v2.group_elems) * 8;
       // phase 1 one block per warp when eight slices fit
       const long long a16   = (lp.v1.asz + 15) / 16;
@@ -378,30 +407,90 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
     for (int i : order)
       all.push_back(cls[c][i]);
   }
-  pl->batch       = batchCount;
-  pl->nhuge       = (int)cls[CLS_HUGE].size();
-  pl->nblock      = (int)cls[CLS_BLOCK].size();
-  pl->nwarp       = (int)cls[CLS_WARP].size();
+  pl->batch  = batchCount;
+  pl->nhuge  = (int)cls[CLS_HUGE].size();
+  pl->nblock = (int)cls[CLS_BLOCK].size();
+  pl->nwarp  = (int)cls[CLS_WARP].size();
+
+  // workspace regions and work items of the huge entries: row items of
+  // about 32k input elements (whole warps' worth of rows), tile items of one
+  // column tile; each list largest first
+  std::vector<VItem> rows, tiles;
+  std::vector<double> rcost, tcost;
+  long long woff = 0;
+  for (int i = 0; i < pl->nhuge; i++)
+  {
+    VDesc &e = all[i];
+    e.woff   = woff;
+    long long Nhead = 1, Ntail = 1, Mtail = 1, Mhead = 1;
+    for (int l = 0; l < e.q; l++)
+    {
+      Nhead *= e.n[l];
+      Mhead *= e.m[l];
+    }
+    for (int l = e.q; l < e.d; l++)
+    {
+      Ntail *= e.n[l];
+      Mtail *= e.m[l];
+    }
+    woff += (Nhead * Mtail + 1) & ~1LL;
+    long long rpi = std::max<long long>(1, 32768 / std::max<long long>(1, Ntail));
+    rpi           = std::max<long long>(VP_WARPS, (rpi + VP_WARPS - 1) / VP_WARPS * VP_WARPS);
+    for (long long h0 = 0; h0 < Nhead; h0 += rpi)
+    {
+      const long long h1 = std::min(Nhead, h0 + rpi);
+      rows.push_back(VItem{i, (int)h0, (int)h1, 0});
+      rcost.push_back((double)(h1 - h0) * (double)(Ntail + Mtail));
+    }
+    const long long nt = (Mtail + e.C - 1) / e.C;
+    for (long long t = 0; t < nt; t++)
+    {
+      tiles.push_back(VItem{i, (int)t, (int)t + 1, 0});
+      tcost.push_back((double)std::min<long long>(e.C, Mtail - t * e.C) * (double)(Nhead + Mhead));
+    }
+  }
+  auto sorted = [](std::vector<VItem> &v, const std::vector<double> &c) {
+    std::vector<int> o(v.size());
+    std::iota(o.begin(), o.end(), 0);
+    std::stable_sort(o.begin(), o.end(), [&](int a, int b) { return c[a] > c[b]; });
+    std::vector<VItem> r;
+    r.reserve(v.size());
+    for (int i : o)
+      r.push_back(v[i]);
+    return r;
+  };
+  std::vector<VItem> items = sorted(rows, rcost);
+  {
+    std::vector<VItem> t = sorted(tiles, tcost);
+    items.insert(items.end(), t.begin(), t.end());
+  }
+  pl->nrow        = (int)rows.size();
+  pl->ntile       = (int)tiles.size();
   pl->flops       = total_flops;
-  pl->slot_elems  = max_slot;
   pl->block_elems = block_elems;
   pl->smem_main   = (size_t)block_elems * 8;
   pl->smem_huge   = std::max<size_t>(smem_huge, 16);
-  pl->huge_grid   = pl->nhuge ? std::min(pl->nhuge, di.sms) : 0;
-  pl->ws_bytes    = (size_t)pl->huge_grid * (size_t)max_slot * 8;
+  pl->ws_bytes    = (size_t)woff * 8;
   pl->exec        = nullptr;
   pl->d_desc      = nullptr;
+  pl->d_items     = nullptr;
   pl->d_counters  = nullptr;
   if (cudaMalloc(&pl->d_counters, 4 * sizeof(int)) != cudaSuccess ||
-      (batchCount > 0 && cudaMalloc(&pl->d_desc, sizeof(VDesc) * batchCount) != cudaSuccess))
+      (batchCount > 0 && cudaMalloc(&pl->d_desc, sizeof(VDesc) * batchCount) != cudaSuccess) ||
+      (!items.empty() && cudaMalloc(&pl->d_items, sizeof(VItem) * items.size()) != cudaSuccess))
   {
+    cudaFree(pl->d_items);
+    cudaFree(pl->d_desc);
     cudaFree(pl->d_counters);
     delete pl;
     return KRON_ERROR_ALLOC;
   }
-  if (batchCount > 0 && cudaMemcpy(pl->d_desc, all.data(), sizeof(VDesc) * batchCount,
-                                   cudaMemcpyHostToDevice) != cudaSuccess)
+  if ((batchCount > 0 && cudaMemcpy(pl->d_desc, all.data(), sizeof(VDesc) * batchCount,
+                                    cudaMemcpyHostToDevice) != cudaSuccess) ||
+      (!items.empty() && cudaMemcpy(pl->d_items, items.data(), sizeof(VItem) * items.size(),
+                                    cudaMemcpyHostToDevice) != cudaSuccess))
   {
+    cudaFree(pl->d_items);
     cudaFree(pl->d_desc);
     cudaFree(pl->d_counters);
     delete pl;
@@ -417,6 +506,7 @@ extern "C" int kron_vplan_destroy(kron_vplan_t plan)
     return KRON_SUCCESS;
   if (plan->exec)
     cudaGraphExecDestroy(plan->exec);
+  cudaFree(plan->d_items);
   cudaFree(plan->d_desc);
   cudaFree(plan->d_counters);
   delete plan;
@@ -434,36 +524,39 @@ static int vplan_launch_all(kron_vplan_t pl, double const *const *A, double **X,
   VParams vp;
   std::memset(&vp, 0, sizeof(vp));
   vp.desc        = pl->d_desc;
+  vp.items       = pl->d_items;
   vp.nhuge       = pl->nhuge;
   vp.nblock      = pl->nblock;
   vp.nwarp       = pl->nwarp;
+  vp.nrow        = pl->nrow;
+  vp.ntile       = pl->ntile;
   vp.counters    = pl->d_counters;
   vp.pA          = A;
   vp.pX          = X;
   vp.pY          = Y;
   vp.ws          = static_cast<double *>(W);
-  vp.slot_elems  = pl->slot_elems;
   vp.block_elems = pl->block_elems;
   void *args[]   = {&vp};
   const int sms  = device_info().sms;
-  if (pl->nhuge > 0)
+  const void *fm = reinterpret_cast<const void *>(&kron_vplan_kernel);
+  const size_t smem = std::max(pl->smem_main, pl->smem_huge);
+  int occ           = 1;
+  if (cached_occupancy(fm, VP_THREADS, smem, &occ) != KRON_SUCCESS)
+    return KRON_ERROR_LAUNCH;
+  const long long work0 =
+      (long long)pl->nrow + pl->nblock + (pl->nwarp + VP_WARPS - 1) / VP_WARPS;
+  if (work0 > 0)
   {
-    const void *fh = reinterpret_cast<const void *>(&kron_vplan_huge_kernel);
-    int occ        = 1;
-    if (cached_occupancy(fh, VP_THREADS, pl->smem_huge, &occ) != KRON_SUCCESS)
-      return KRON_ERROR_LAUNCH;
-    if (cudaLaunchKernel(fh, dim3(pl->huge_grid), dim3(VP_THREADS), args, pl->smem_huge, s) !=
-        cudaSuccess)
+    vp.stage       = 0;
+    const int grid = (int)std::max<long long>(1, std::min<long long>((long long)sms * occ, work0));
+    if (cudaLaunchKernel(fm, dim3(grid), dim3(VP_THREADS), args, smem, s) != cudaSuccess)
       return KRON_ERROR_LAUNCH;
   }
-  if (pl->nblock + pl->nwarp > 0)
+  if (pl->ntile > 0)
   {
-    const void *fm = reinterpret_cast<const void *>(&kron_vplan_kernel);
-    int occ        = 1;
-    if (cached_occupancy(fm, VP_THREADS, pl->smem_main, &occ) != KRON_SUCCESS)
-      return KRON_ERROR_LAUNCH;
-    const int grid = std::max(1, std::min(sms * occ, pl->nblock + (pl->nwarp + VP_WARPS - 1) / VP_WARPS));
-    if (cudaLaunchKernel(fm, dim3(grid), dim3(VP_THREADS), args, pl->smem_main, s) != cudaSuccess)
+    vp.stage       = 1;
+    const int grid = std::max(1, std::min(sms * occ, pl->ntile));
+    if (cudaLaunchKernel(fm, dim3(grid), dim3(VP_THREADS), args, smem, s) != cudaSuccess)
       return KRON_ERROR_LAUNCH;
   }
   return KRON_SUCCESS;
