@@ -77,30 +77,70 @@ __device__ __forceinline__ T ldg_stream(const T *p)
 template <typename T>
 __device__ __forceinline__ void group_copy_in(T *dst, const T *src, int count, int t, int GS)
 {
+  // B loads of a thread are issued before its stores: with generic
+  // pointers every load would otherwise wait behind the previous store
+  constexpr int B = 8;
   constexpr int V = 16 / sizeof(T);
   const bool vec  = ((reinterpret_cast<uintptr_t>(src) & 15) == 0) && (count % V == 0);
   if (vec)
   {
-    const int nv = count / V;
-    if constexpr (sizeof(T) == 8)
+    using VT      = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+    constexpr int BV = B / 2;
+    const int nv  = count / V;
+    const VT *s   = reinterpret_cast<const VT *>(src);
+    VT *d         = reinterpret_cast<VT *>(dst);
+    for (int i0 = t; i0 < nv; i0 += GS * BV)
     {
-      const double2 *s = reinterpret_cast<const double2 *>(src);
-      double2 *d       = reinterpret_cast<double2 *>(dst);
-      for (int i = t; i < nv; i += GS)
-        d[i] = __ldg(s + i);
-    }
-    else
-    {
-      const float4 *s = reinterpret_cast<const float4 *>(src);
-      float4 *d       = reinterpret_cast<float4 *>(dst);
-      for (int i = t; i < nv; i += GS)
-        d[i] = __ldg(s + i);
+      VT v[BV];
+#pragma unroll
+      for (int b = 0; b < BV; b++)
+        if (i0 + b * GS < nv)
+          v[b] = __ldg(s + i0 + b * GS);
+#pragma unroll
+      for (int b = 0; b < BV; b++)
+        if (i0 + b * GS < nv)
+          d[i0 + b * GS] = v[b];
     }
   }
   else
   {
-    for (int i = t; i < count; i += GS)
-      dst[i] = __ldg(src + i);
+    for (int i0 = t; i0 < count; i0 += GS * B)
+    {
+      T v[B];
+#pragma unroll
+      for (int b = 0; b < B; b++)
+        if (i0 + b * GS < count)
+          v[b] = __ldg(src + i0 + b * GS);
+#pragma unroll
+      for (int b = 0; b < B; b++)
+        if (i0 + b * GS < count)
+          dst[i0 + b * GS] = v[b];
+    }
+  }
+}
+
+// A tile of `rows` rows x C columns (row stride in_row, the first Cc columns
+// valid, the rest zero-filled) into dst, loads batched as above.
+template <typename T>
+__device__ __forceinline__ void group_copy_tile(T *dst, const T *src, int rows, int C, int Cc,
+                                                long long in_row, int t, int GS)
+{
+  constexpr int B = 8;
+  const int count = rows * C;
+  for (int q0 = t; q0 < count; q0 += GS * B)
+  {
+    T v[B];
+#pragma unroll
+    for (int b = 0; b < B; b++)
+    {
+      const int q = q0 + b * GS;
+      const int h = q / C, c = q - (q / C) * C;
+      v[b]        = (q < count && c < Cc) ? __ldg(src + h * in_row + c) : T(0);
+    }
+#pragma unroll
+    for (int b = 0; b < B; b++)
+      if (q0 + b * GS < count)
+        dst[q0 + b * GS] = v[b];
   }
 }
 
@@ -615,11 +655,7 @@ __global__ void __launch_bounds__(256) kron_gen_kernel(const __grid_constant__ P
       if (v.C == 1)
         group_copy_in(b0, in, rows_in, t, GS);
       else
-        for (int q = t; q < rows_in * v.C; q += GS)
-        {
-          const int h = q / v.C, c = q - h * v.C;
-          b0[q]       = (c < Cc) ? __ldg(in + h * v.in_row + c) : T(0);
-        }
+        group_copy_tile(b0, in, rows_in, v.C, Cc, v.in_row, t, GS);
       group_sync(g, GS);
 
       T *cur = b0, *nxt = b1;

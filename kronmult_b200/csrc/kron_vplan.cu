@@ -38,7 +38,8 @@ namespace {
 constexpr int VP_THREADS  = 256;
 constexpr int VP_WARPS    = VP_THREADS / 32;
 constexpr int WARP_MAX    = 512;   // elements of the largest intermediate, warp class
-constexpr int CLS_WARP    = 0, CLS_BLOCK = 1, CLS_HUGE = 2;
+constexpr int CLS_WARP = 0, CLS_QUAD = 1, CLS_HALF = 2, CLS_BLOCK = 3, CLS_HUGE = 4;
+constexpr int NCLS     = 5;
 
 struct VDesc
 {
@@ -62,9 +63,9 @@ struct VItem
 
 struct VParams
 {
-  const VDesc *desc;          // [huge | block | warp]
+  const VDesc *desc;          // [huge | block | half | quad | warp]
   const VItem *items;         // [row items | tile items]
-  int nhuge, nblock, nwarp;
+  int nhuge, nblock, nhalf, nquad, nwarp;
   int nrow, ntile;
   int stage;                  // 0: row items, block and warp classes; 1: tile items
   int *counters;              // work counters (zeroed before every execution)
@@ -80,8 +81,10 @@ struct VParams
 __device__ __forceinline__ void vp_group_entry(const GenView &v, bool strided, const double *x,
                                                double *out, int accum, double *b0, double *b1,
                                                double *As, const double *const *A,
-                                               const int *ld, int t, int GS, int g)
+                                               const int *ld, int t, int GS, int g,
+                                               bool load_a = true)
 {
+  if (load_a)
   {
     int o = 0;
     for (int q = 0; q < v.dd; q++)
@@ -104,11 +107,7 @@ __device__ __forceinline__ void vp_group_entry(const GenView &v, bool strided, c
   if (!strided)
     group_copy_in(b0, x, rows_in, t, GS);
   else
-    for (int q = t; q < rows_in * v.C; q += GS)
-    {
-      const int h = q / v.C, c = q - h * v.C;
-      b0[q]       = (c < v.total_cols) ? __ldg(x + h * v.in_row + c) : 0.0;
-    }
+    group_copy_tile(b0, x, rows_in, v.C, (int)v.total_cols, v.in_row, t, GS);
   group_sync(g, GS);
   double *cur = b0, *nxt = b1;
   gen_apply_modes<double, PREC_F64>(v, cur, nxt, As, v.C, t, GS, g);
@@ -182,13 +181,46 @@ __device__ __forceinline__ int block_take(int *counter, int *s_idx, int tid)
   return idx;
 }
 
-// Stage 0: huge row items, block class, warp class.  Stage 1: huge tile
-// items.  Counters: [0] row items, [1] block class, [2] warp class,
-// [3] tile items.
-__global__ void __launch_bounds__(VP_THREADS, 1) kron_vplan_kernel(const __grid_constant__ VParams vp)
+// Entries of one class run by groups of GS threads, VP_THREADS / GS per
+// block, each group with its own slice of shared memory and named barrier.
+template <int GS>
+__device__ __forceinline__ void group_class(const VParams &vp, const VDesc *list, int n,
+                                            int *counter, double *smem, int *s_gidx, int tid)
+{
+  constexpr int NG = VP_THREADS / GS;
+  const int g = tid / GS, t = tid - (tid / GS) * GS;
+  double *b0  = smem + (long long)g * ((vp.block_elems / NG) & ~1);
+  const double *A[6];
+  int ld[6];
+  const double *x;
+  double *y;
+  while (true)
+  {
+    if (t == 0)
+      s_gidx[g] = atomicAdd(counter, 1);
+    group_sync(g, GS);
+    const int idx = s_gidx[g];
+    group_sync(g, GS);
+    if (idx >= n)
+      break;
+    const VDesc e = list[idx];
+    GenView v;
+    vp_view(v, e, 0, e.d);
+    vp_operands(vp, e, A, ld, x, y);
+    const int mi = (e.mi + 1) & ~1;
+    vp_group_entry(v, false, x, y, ACC_ATOMIC, b0, b0 + mi, b0 + 2 * mi, A, ld, t, GS, g);
+  }
+  __syncthreads(); // the next class lays its slices over these
+}
+
+// Stage 0: huge row items, then the block, half, quad and warp classes.
+// Stage 1: huge tile items.  Counters: [0] row items, [1] block class,
+// [2] warp class, [3] tile items, [4] half class, [5] quad class.
+__global__ void __launch_bounds__(VP_THREADS, 2) kron_vplan_kernel(const __grid_constant__ VParams vp)
 {
   extern __shared__ __align__(16) double smem[];
   __shared__ int s_idx;
+  __shared__ int s_gidx[4];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const double *A[6];
   int ld[6];
@@ -245,14 +277,17 @@ __global__ void __launch_bounds__(VP_THREADS, 1) kron_vplan_kernel(const __grid_
       // one head row per warp (the plan checked that eight slices fit)
       const int slice = (2 * mi1 + e.pad[1] * 16 + 1) & ~1;
       double *b0      = smem + warp * slice;
+      // the warp's factors stay in its slice from its first row on
       for (int h = it.lo + warp; h < it.hi; h += VP_WARPS)
         vp_group_entry(v1, false, x + (long long)h * hd.Ntail, wr + (long long)h * hd.Mtail,
-                       ACC_STORE, b0, b0 + mi1, b0 + 2 * mi1, A, ld, lane, 32, warp);
+                       ACC_STORE, b0, b0 + mi1, b0 + 2 * mi1, A, ld, lane, 32, warp,
+                       h == it.lo + warp);
     }
     else
       for (int h = it.lo; h < it.hi; h++)
         vp_group_entry(v1, false, x + (long long)h * hd.Ntail, wr + (long long)h * hd.Mtail,
-                       ACC_STORE, smem, smem + mi1, smem + 2 * mi1, A, ld, tid, VP_THREADS, 0);
+                       ACC_STORE, smem, smem + mi1, smem + 2 * mi1, A, ld, tid, VP_THREADS, 0,
+                       h == it.lo);
     __syncthreads();
   }
 
@@ -272,10 +307,17 @@ __global__ void __launch_bounds__(VP_THREADS, 1) kron_vplan_kernel(const __grid_
                    VP_THREADS, 0);
   }
 
+  // ---- half and quad classes: two / four entries per block at a time
+  {
+    const VDesc *hd = vp.desc + vp.nhuge + vp.nblock;
+    group_class<VP_THREADS / 2>(vp, hd, vp.nhalf, &vp.counters[4], smem, s_gidx, tid);
+    group_class<VP_THREADS / 4>(vp, hd + vp.nhalf, vp.nquad, &vp.counters[5], smem, s_gidx, tid);
+  }
+
   // ---- warp class: one warp per entry
   const int slice = vp.block_elems / VP_WARPS;
   double *b0      = smem + warp * slice;
-  const VDesc *wd = vp.desc + vp.nhuge + vp.nblock;
+  const VDesc *wd = vp.desc + vp.nhuge + vp.nblock + vp.nhalf + vp.nquad;
   while (true)
   {
     int idx = 0;
@@ -298,14 +340,14 @@ __global__ void __launch_bounds__(VP_THREADS, 1) kron_vplan_kernel(const __grid_
 struct kron_vplan_st
 {
   int batch;
-  int nhuge, nblock, nwarp;
+  int nhuge, nblock, nhalf, nquad, nwarp;
   int nrow, ntile;
   VDesc *d_desc;
   VItem *d_items;
   int *d_counters;
   double flops;
   size_t ws_bytes;
-  size_t smem_main, smem_huge;
+  size_t smem_main, smem_huge, smem_tile;
   int block_elems;
   // graph cache
   cudaGraphExec_t exec;
@@ -322,10 +364,11 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
   const int maxsm      = di.max_smem_optin;
   // block class: two buffers + factors within the block's shared memory
   const int block_elems = (maxsm - 4096) / 8;
-  std::vector<VDesc> cls[3];
-  std::vector<double> cost[3];
+  std::vector<VDesc> cls[NCLS];
+  std::vector<double> cost[NCLS];
   double total_flops   = 0.0;
   size_t smem_huge     = 0;
+  size_t smem_tile     = 0;
   for (int k = 0; k < batchCount; k++)
   {
     const int *s = shapes + 13LL * k;
@@ -356,9 +399,14 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
       asz += (long long)m[l] * n[l];
     const long long mi2r = (mi + 1) & ~1LL;
     int c;
+    const long long need = 2 * mi2r + asz;
     if (mi <= WARP_MAX && 2 * WARP_MAX + asz <= block_elems / VP_WARPS)
       c = CLS_WARP;
-    else if (2 * mi2r + asz <= block_elems)
+    else if (need <= ((block_elems / 4) & ~1))
+      c = CLS_QUAD;
+    else if (need <= ((block_elems / 2) & ~1))
+      c = CLS_HALF;
+    else if (need <= block_elems)
       c = CLS_BLOCK;
     else
     {
@@ -367,10 +415,20 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
       if (!plan_large(d, m, n, 8, false, lp) || lp.C > 255)
         return KRON_ERROR_NOT_SUPPORTED;
       e.q    = (unsigned char)lp.q;
-      e.C    = (unsigned char)lp.C;
       e.fwd1 = (unsigned char)lp.v1.forward;
       e.fwd2 = (unsigned char)lp.v2.forward;
-      e.mi2  = lp.v2.max_inter; // rows x C, rounded
+      // phase-2 tiles narrowed so that one fits half the shared memory (two
+      // blocks per SM run the tile launch)
+      {
+        const long long rows2 = std::max<long long>(1, lp.v2.max_inter / std::max(1, lp.C));
+        const long long budget = (long long)(maxsm / 2 - 1024) / 8 - lp.v2.asz;
+        long long C2 = std::min<long long>(lp.C, budget / (2 * rows2));
+        if (C2 < 1)
+          C2 = lp.C; // keep the plan's width; the tile launch then runs one block per SM
+        e.C   = (unsigned char)C2;
+        e.mi2 = (int)((rows2 * C2 + 1) & ~1LL);
+        smem_tile = std::max(smem_tile, (size_t)(2 * e.mi2 + lp.v2.asz + 2) * 8);
+      }
       size_t need = (size_t)std::max(lp.v1.group_elems, lp.v2.group_elems) * 8;
       // phase 1 one block per warp when eight slices fit
       const long long a16   = (lp.v1.asz + 15) / 16;
@@ -398,7 +456,7 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
     return KRON_ERROR_ALLOC;
   std::vector<VDesc> all;
   all.reserve(batchCount);
-  for (int c : {CLS_HUGE, CLS_BLOCK, CLS_WARP})
+  for (int c : {CLS_HUGE, CLS_BLOCK, CLS_HALF, CLS_QUAD, CLS_WARP})
   {
     std::vector<int> order(cls[c].size());
     std::iota(order.begin(), order.end(), 0);
@@ -410,6 +468,8 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
   pl->batch  = batchCount;
   pl->nhuge  = (int)cls[CLS_HUGE].size();
   pl->nblock = (int)cls[CLS_BLOCK].size();
+  pl->nhalf  = (int)cls[CLS_HALF].size();
+  pl->nquad  = (int)cls[CLS_QUAD].size();
   pl->nwarp  = (int)cls[CLS_WARP].size();
 
   // workspace regions and work items of the huge entries: row items of
@@ -470,12 +530,13 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
   pl->block_elems = block_elems;
   pl->smem_main   = (size_t)block_elems * 8;
   pl->smem_huge   = std::max<size_t>(smem_huge, 16);
+  pl->smem_tile   = std::max<size_t>(smem_tile, 16);
   pl->ws_bytes    = (size_t)woff * 8;
   pl->exec        = nullptr;
   pl->d_desc      = nullptr;
   pl->d_items     = nullptr;
   pl->d_counters  = nullptr;
-  if (cudaMalloc(&pl->d_counters, 4 * sizeof(int)) != cudaSuccess ||
+  if (cudaMalloc(&pl->d_counters, 8 * sizeof(int)) != cudaSuccess ||
       (batchCount > 0 && cudaMalloc(&pl->d_desc, sizeof(VDesc) * batchCount) != cudaSuccess) ||
       (!items.empty() && cudaMalloc(&pl->d_items, sizeof(VItem) * items.size()) != cudaSuccess))
   {
@@ -519,7 +580,7 @@ extern "C" double kron_vplan_flops(kron_vplan_t plan) { return plan ? plan->flop
 static int vplan_launch_all(kron_vplan_t pl, double const *const *A, double **X, double **Y,
                             void *W, cudaStream_t s)
 {
-  if (cudaMemsetAsync(pl->d_counters, 0, 4 * sizeof(int), s) != cudaSuccess)
+  if (cudaMemsetAsync(pl->d_counters, 0, 8 * sizeof(int), s) != cudaSuccess)
     return KRON_ERROR_LAUNCH;
   VParams vp;
   std::memset(&vp, 0, sizeof(vp));
@@ -527,6 +588,8 @@ static int vplan_launch_all(kron_vplan_t pl, double const *const *A, double **X,
   vp.items       = pl->d_items;
   vp.nhuge       = pl->nhuge;
   vp.nblock      = pl->nblock;
+  vp.nhalf       = pl->nhalf;
+  vp.nquad       = pl->nquad;
   vp.nwarp       = pl->nwarp;
   vp.nrow        = pl->nrow;
   vp.ntile       = pl->ntile;
@@ -543,8 +606,8 @@ static int vplan_launch_all(kron_vplan_t pl, double const *const *A, double **X,
   int occ           = 1;
   if (cached_occupancy(fm, VP_THREADS, smem, &occ) != KRON_SUCCESS)
     return KRON_ERROR_LAUNCH;
-  const long long work0 =
-      (long long)pl->nrow + pl->nblock + (pl->nwarp + VP_WARPS - 1) / VP_WARPS;
+  const long long work0 = (long long)pl->nrow + pl->nblock + (pl->nhalf + 1) / 2 +
+                          (pl->nquad + 3) / 4 + (pl->nwarp + VP_WARPS - 1) / VP_WARPS;
   if (work0 > 0)
   {
     vp.stage       = 0;
@@ -554,9 +617,13 @@ static int vplan_launch_all(kron_vplan_t pl, double const *const *A, double **X,
   }
   if (pl->ntile > 0)
   {
-    vp.stage       = 1;
-    const int grid = std::max(1, std::min(sms * occ, pl->ntile));
-    if (cudaLaunchKernel(fm, dim3(grid), dim3(VP_THREADS), args, smem, s) != cudaSuccess)
+    vp.stage   = 1;
+    int occ1   = 1;
+    if (cached_occupancy(fm, VP_THREADS, pl->smem_tile, &occ1) != KRON_SUCCESS)
+      return KRON_ERROR_LAUNCH;
+    const int grid = std::max(1, std::min(sms * occ1, pl->ntile));
+    if (cudaLaunchKernel(fm, dim3(grid), dim3(VP_THREADS), args, pl->smem_tile, s) !=
+        cudaSuccess)
       return KRON_ERROR_LAUNCH;
   }
   return KRON_SUCCESS;
