@@ -280,6 +280,23 @@ int kron_measure_fp64_peak(double *tensor_tflops, double *cuda_core_tflops);
 int kron_device_status(int clear);
 
 /* ------------------------------------------------------------------------
+ * Pointer arrays built on the device from integer lists (no reference
+ * counterpart; the reference's tests build them on the host and copy them,
+ * test_kronmult6_xbatched.cpp:231-271).  All arrays are device arrays;
+ * a NULL list means the identity (entry k, or block l + k*d):
+ *   Xarray_out[k]         = X + xlist[k] * xstride
+ *   Yarray_out[k]         = Y + ylist[k] * ystride
+ *   Aarray_out[l + k * d] = A + alist[l + k * d] * astride
+ * Any output may be NULL (not built).  Indices are not range-checked.
+ * Asynchronous on `stream`.
+ * ---------------------------------------------------------------------- */
+int kron_build_pointers_async(int d, int batchCount, double const *A, long long astride,
+                              int const alist[], double const *X, long long xstride,
+                              int const xlist[], double *Y, long long ystride,
+                              int const ylist[], double const *Aarray_out[],
+                              double *Xarray_out[], double *Yarray_out[], kron_stream_t stream);
+
+/* ------------------------------------------------------------------------
  * Autotuner (no reference counterpart).  For square shapes the library picks
  * among kernel variants, each with one tuning parameter:
  *   KRON_VARIANT_MMA8   FP64 tensor-core kernel for d = 3, n = 8

@@ -77,6 +77,8 @@ def _sig(lib):
     S["kron_version"] = []
     S["kron_measure_fp64_peak"] = [_vp, _vp]
     S["kron_device_status"] = [_i]
+    S["kron_build_pointers_async"] = [_i, _i, _vp, C.c_longlong, _vp, _vp, C.c_longlong, _vp,
+                                      _vp, C.c_longlong, _vp, _vp, _vp, _vp, _vp]
     S["kron_autotune"] = [_i, _i, _i, _i, _vp, _vp, _vp, _vp]
     S["kron_tune_set"] = [_i, _i, _i, _i, _i]
     S["kron_tune_get"] = [_i, _i, _i, _vp, _vp]
@@ -197,6 +199,24 @@ def measure_fp64_peak():
     a, b = C.c_double(), C.c_double()
     _check(lib().kron_measure_fp64_peak(C.byref(a), C.byref(b)), "kron_measure_fp64_peak")
     return a.value, b.value
+
+
+def build_pointers(d, A, astride, alist, X, xstride, xlist, Y, ystride, ylist, stream=None):
+    """Device pointer arrays (pA, pX, pY) of the xbatched / pbatched layouts
+    from device int32 index lists (None: identity):
+    pX[k] = X + xlist[k]*xstride, pY[k] = Y + ylist[k]*ystride,
+    pA[l + k*d] = A + alist[l + k*d]*astride (strides in elements)."""
+    torch = _torch()
+    batch = next(v.numel() for v in (xlist, ylist) if v is not None) if (
+        xlist is not None or ylist is not None) else alist.numel() // d
+    pA = torch.empty(batch * d, dtype=torch.int64, device="cuda")
+    pX = torch.empty(batch, dtype=torch.int64, device="cuda")
+    pY = torch.empty(batch, dtype=torch.int64, device="cuda")
+    _check(lib().kron_build_pointers_async(d, batch, _ptr(A), astride, _ptr(alist), _ptr(X),
+                                           xstride, _ptr(xlist), _ptr(Y), ystride, _ptr(ylist),
+                                           _ptr(pA), _ptr(pX), _ptr(pY), _stream(stream)),
+           "kron_build_pointers")
+    return pA, pX, pY
 
 
 # ---------------------------------------------------------------- autotuner

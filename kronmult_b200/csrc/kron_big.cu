@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdlib>
+#include <type_traits>
 
 #include "kron_launch.h"
 #include "kron_mma8_core.cuh"
@@ -118,7 +119,13 @@ __device__ __forceinline__ void cp_async_elem(T *dst, const T *src)
   else
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+  unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ bool al16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 template <int Nleft>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(Nleft) : "memory"); }
 
@@ -298,11 +305,16 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
     {
       // rounds of NB consecutive head rows, loads double buffered (cp.async)
       constexpr int NB = S::NB;
+      constexpr int V = 16 / sizeof(T); // elements per 16-byte copy
       auto issue_round = [&](int h0, T *buf) {
         const int nr  = min(NB, he - h0);
         const T *src = en.x + (long long)h0 * LT;
-        for (int q = tid; q < nr * LT; q += BIG_THREADS)
-          cp_async_elem(buf + q, src + q);
+        if ((LT * sizeof(T)) % 16 == 0 && al16(src))
+          for (int q = tid; q < nr * LT / V; q += BIG_THREADS)
+            cp_async16(buf + q * V, src + q * V);
+        else
+          for (int q = tid; q < nr * LT; q += BIG_THREADS)
+            cp_async_elem(buf + q, src + q);
         cp_commit();
       };
       int cur = 0;
@@ -322,8 +334,15 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
         const int nr = min(NB, he - h0);
         round_tail_passes<T, D, N, Q, Q>(buf, nr, As, tid);
         T *dst = w + (long long)h0 * LT;
-        for (int q = tid; q < nr * LT; q += BIG_THREADS)
-          dst[q] = buf[q];
+        if ((LT * sizeof(T)) % 16 == 0 && al16(dst))
+        {
+          using VT = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+          for (int q = tid; q < nr * LT / V; q += BIG_THREADS)
+            reinterpret_cast<VT *>(dst)[q] = reinterpret_cast<const VT *>(buf)[q];
+        }
+        else
+          for (int q = tid; q < nr * LT; q += BIG_THREADS)
+            dst[q] = buf[q];
         __syncthreads();
         cur ^= 1;
       }
@@ -413,16 +432,37 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
     }
     else
     {
+      constexpr int V = 16 / sizeof(T); // elements per 16-byte copy
+      // W rows are 16-byte aligned when the slot is and rows are whole
+      // 16-byte multiples (tile starts c0 are multiples of C)
+      const bool wvec = (LT * sizeof(T)) % 16 == 0 && (C % V) == 0 && al16(w);
       auto issue_tile = [&](int tt, T *buf) {
         const int c0 = tt * C, cc = min(C, LT - c0);
-        for (int q = tid; q < LH * C; q += BIG_THREADS)
-        {
-          const int h = q / C, c = q - (q / C) * C;
-          if (c < cc)
-            cp_async_elem(buf + q, w + (long long)h * LT + c0 + c);
-          else
-            buf[q] = T(0);
-        }
+        if (wvec)
+          for (int q = tid; q < LH * C / V; q += BIG_THREADS)
+          {
+            const int h = (q * V) / C, c = q * V - h * C;
+            if (c + V <= cc)
+              cp_async16(buf + q * V, w + (long long)h * LT + c0 + c);
+            else
+#pragma unroll
+              for (int u = 0; u < V; u++)
+              {
+                if (c + u < cc)
+                  cp_async_elem(buf + q * V + u, w + (long long)h * LT + c0 + c + u);
+                else
+                  buf[q * V + u] = T(0);
+              }
+          }
+        else
+          for (int q = tid; q < LH * C; q += BIG_THREADS)
+          {
+            const int h = q / C, c = q - (q / C) * C;
+            if (c < cc)
+              cp_async_elem(buf + q, w + (long long)h * LT + c0 + c);
+            else
+              buf[q] = T(0);
+          }
         cp_commit();
       };
       int cur = 0;
