@@ -486,17 +486,22 @@ class XbatchedBig(Workload):
         return float(self.cs) * 2 * self.d * self.n ** (self.d + 1)
 
 
-def make_workload(cfg, precision):
+def make_workload(cfg, precision, entries=0):
+    """The workload of --config cfg; entries > 0 scales its batch down (or
+    up) for small profiling cases (configs 1, 3 and 5; outputs of config 5
+    keep their 716:1024 ratio)."""
     if cfg == 1:
-        return BatchedSquare(6, 4, 512, "f64", "uniform")
+        return BatchedSquare(6, 4, entries or 512, "f64", "uniform")
     if cfg == 2:
         return XbatchedOverlap()
     if cfg == 3:
         n = int(os.environ.get("KRON_BENCH_N", "4"))
-        return BatchedSquare(6, n, 4096, precision, "normal")
+        return BatchedSquare(6, n, entries or 4096, precision, "normal")
     if cfg == 4:
         return UnevenBatch()
     if cfg == 5:
+        if entries:
+            return XbatchedBig(batch=entries, nout=max(1, entries * 716 // 1024))
         return XbatchedBig()
     raise SystemExit(f"--config {cfg} not available in this bench")
 
@@ -523,6 +528,8 @@ def profile_key(args):
     n = os.environ.get("KRON_BENCH_N")
     if args.config == 3 and n and n != "4":
         key += f"-n{n}"
+    if getattr(args, "entries", 0):
+        key += f"-e{args.entries}"
     return key
 
 
@@ -602,7 +609,7 @@ def run_reference(args, world, rank):
         return
     import oracle
 
-    wl = make_workload(args.config, args.precision)
+    wl = make_workload(args.config, args.precision, args.entries)
     if oracle.Reference.available("recur"):
         ref = oracle.Reference("recur")
         kind = "reference"
@@ -650,7 +657,7 @@ def run_ours(args, world, rank, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     kb.lib()
-    wl = make_workload(args.config, args.precision)
+    wl = make_workload(args.config, args.precision, args.entries)
     wl.setup(torch, kb, args.mode)
     flush_w = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     flush_r = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -833,6 +840,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--entries", type=int, default=0,
+                    help="scale the batch of configs 1/3/5 (small profiling cases)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
