@@ -593,6 +593,18 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+def max_over_ranks(dist, values, device):
+    """Element-wise max of `values` over all ranks (the slowest replica sets
+    every time); the values unchanged without a process group."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -729,10 +741,7 @@ def run_ours(args, world, rank, local):
     e2e_ms = e_s.elapsed_time(e_e)
     clocks = clock.stop() if clock else None
 
-    if dist is not None:
-        t = torch.tensor([tot_ms, e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms, e2e_ms = t.tolist()
+    tot_ms, e2e_ms = max_over_ranks(dist, [tot_ms, e2e_ms], "cuda")
 
     # CPU baseline (rank 0, N=1 only): the reference's OpenMP build, bounded sample
     cpu = None
