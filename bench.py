@@ -243,7 +243,16 @@ class BatchedSquare(Workload):
         self.dY = torch.zeros(self.L * self.batch, dtype=dt, device=dev)
         need = kb.lib().kron_batched_workspace_bytes(self.d, self.n, self.batch)
         self.dW = torch.empty(max(1, need // 8), dtype=dt, device=dev) if need else None
-        self.launches_per_step = 2 if need else 1
+        # vectors beyond shared memory: one cluster-kernel launch for
+        # d=6 n=6..8 (FP64) / n=7..8 (FP32) and d=5 n=8 (FP64), else the
+        # two-phase path's two launches
+        if not need:
+            self.launches_per_step = 1
+        else:
+            d, n = self.d, self.n
+            fp64 = self.precision == "f64"
+            cluster = (d == 6 and (6 if fp64 else 7) <= n <= 8) or (fp64 and d == 5 and n == 8)
+            self.launches_per_step = 1 if cluster else 2
         self.h = {k: v.cpu().pin_memory() for k, v in dict(A=self.dA, X=self.dX,
                                                           Y=self.dY).items()}
         self.hYout = torch.empty_like(self.h["Y"]).pin_memory()
