@@ -297,6 +297,20 @@ int kron_build_pointers_async(int d, int batchCount, double const *A, long long 
                               double *Xarray_out[], double *Yarray_out[], kron_stream_t stream);
 
 /* ------------------------------------------------------------------------
+ * Repeated application with a fixed operand (no reference counterpart): an
+ * iterative solver applies the same kron(A_1..A_d) to a new X every
+ * iteration.  kron_l2_persist_async keeps [ptr, ptr + bytes) -- typically A
+ * -- resident in L2 for the kernels launched on `stream` afterwards (a
+ * persisting access-policy window on the stream, also captured into graphs
+ * with the kernels; this context's persisting L2 carve-out is set to the
+ * window, capped at the device maximum).  kron_l2_persist_reset clears the
+ * window, returns the lines to normal and the carve-out to 0.  Both settings
+ * end with the process.
+ * ---------------------------------------------------------------------- */
+int kron_l2_persist_async(const void *ptr, size_t bytes, kron_stream_t stream);
+int kron_l2_persist_reset(kron_stream_t stream);
+
+/* ------------------------------------------------------------------------
  * Autotuner (no reference counterpart).  For square shapes the library picks
  * among kernel variants, each with one tuning parameter:
  *   KRON_VARIANT_MMA8   FP64 tensor-core kernel for d = 3, n = 8

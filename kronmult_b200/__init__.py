@@ -79,6 +79,8 @@ def _sig(lib):
     S["kron_device_status"] = [_i]
     S["kron_build_pointers_async"] = [_i, _i, _vp, C.c_longlong, _vp, _vp, C.c_longlong, _vp,
                                       _vp, C.c_longlong, _vp, _vp, _vp, _vp, _vp]
+    S["kron_l2_persist_async"] = [_vp, _sz, _vp]
+    S["kron_l2_persist_reset"] = [_vp]
     S["kron_autotune"] = [_i, _i, _i, _i, _vp, _vp, _vp, _vp]
     S["kron_tune_set"] = [_i, _i, _i, _i, _i]
     S["kron_tune_get"] = [_i, _i, _i, _vp, _vp]
@@ -217,6 +219,17 @@ def build_pointers(d, A, astride, alist, X, xstride, xlist, Y, ystride, ylist, s
                                            _ptr(pA), _ptr(pX), _ptr(pY), _stream(stream)),
            "kron_build_pointers")
     return pA, pX, pY
+
+
+def l2_persist(t, stream=None):
+    """Keep tensor t (e.g. the factors A of a repeated apply) resident in L2
+    for the library's kernels on `stream`."""
+    _check(lib().kron_l2_persist_async(_ptr(t), t.numel() * t.element_size(), _stream(stream)),
+           "kron_l2_persist")
+
+
+def l2_persist_reset(stream=None):
+    _check(lib().kron_l2_persist_reset(_stream(stream)), "kron_l2_persist_reset")
 
 
 # ---------------------------------------------------------------- autotuner

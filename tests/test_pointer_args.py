@@ -26,3 +26,8 @@ def test_output_without_base_is_rejected():
 def test_nothing_to_build_is_success():
     assert kb.lib().kron_build_pointers_async(3, 0, None, 1, None, None, 1, None, None, 1, None,
                                               None, None, None, None) == 0
+
+
+def test_l2_persist_rejects_empty_range():
+    assert kb.lib().kron_l2_persist_async(None, 1024, None) == 1
+    assert kb.lib().kron_l2_persist_async(C.c_void_p(256), 0, None) == 1
