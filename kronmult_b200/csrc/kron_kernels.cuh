@@ -77,70 +77,34 @@ __device__ __forceinline__ T ldg_stream(const T *p)
 template <typename T>
 __device__ __forceinline__ void group_copy_in(T *dst, const T *src, int count, int t, int GS)
 {
-  // B loads of a thread are issued before its stores: with generic
-  // pointers every load would otherwise wait behind the previous store
-  constexpr int B = 8;
   constexpr int V = 16 / sizeof(T);
   const bool vec  = ((reinterpret_cast<uintptr_t>(src) & 15) == 0) && (count % V == 0);
   if (vec)
   {
-    using VT      = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
-    constexpr int BV = B / 2;
-    const int nv  = count / V;
-    const VT *s   = reinterpret_cast<const VT *>(src);
-    VT *d         = reinterpret_cast<VT *>(dst);
-    for (int i0 = t; i0 < nv; i0 += GS * BV)
-    {
-      VT v[BV];
-#pragma unroll
-      for (int b = 0; b < BV; b++)
-        if (i0 + b * GS < nv)
-          v[b] = __ldg(s + i0 + b * GS);
-#pragma unroll
-      for (int b = 0; b < BV; b++)
-        if (i0 + b * GS < nv)
-          d[i0 + b * GS] = v[b];
-    }
+    using VT     = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+    const int nv = count / V;
+    const VT *s  = reinterpret_cast<const VT *>(src);
+    VT *d        = reinterpret_cast<VT *>(dst);
+    for (int i = t; i < nv; i += GS)
+      d[i] = __ldg(s + i);
   }
   else
   {
-    for (int i0 = t; i0 < count; i0 += GS * B)
-    {
-      T v[B];
-#pragma unroll
-      for (int b = 0; b < B; b++)
-        if (i0 + b * GS < count)
-          v[b] = __ldg(src + i0 + b * GS);
-#pragma unroll
-      for (int b = 0; b < B; b++)
-        if (i0 + b * GS < count)
-          dst[i0 + b * GS] = v[b];
-    }
+    for (int i = t; i < count; i += GS)
+      dst[i] = __ldg(src + i);
   }
 }
 
 // A tile of `rows` rows x C columns (row stride in_row, the first Cc columns
-// valid, the rest zero-filled) into dst, loads batched as above.
+// valid, the rest zero-filled) into dst.
 template <typename T>
 __device__ __forceinline__ void group_copy_tile(T *dst, const T *src, int rows, int C, int Cc,
                                                 long long in_row, int t, int GS)
 {
-  constexpr int B = 8;
-  const int count = rows * C;
-  for (int q0 = t; q0 < count; q0 += GS * B)
+  for (int q = t; q < rows * C; q += GS)
   {
-    T v[B];
-#pragma unroll
-    for (int b = 0; b < B; b++)
-    {
-      const int q = q0 + b * GS;
-      const int h = q / C, c = q - (q / C) * C;
-      v[b]        = (q < count && c < Cc) ? __ldg(src + h * in_row + c) : T(0);
-    }
-#pragma unroll
-    for (int b = 0; b < B; b++)
-      if (q0 + b * GS < count)
-        dst[q0 + b * GS] = v[b];
+    const int h = q / C, c = q - (q / C) * C;
+    dst[q]      = (c < Cc) ? __ldg(src + h * in_row + c) : T(0);
   }
 }
 
@@ -496,7 +460,10 @@ __device__ __forceinline__ bool gen_mode_sized(int nq, int mq, const T *cur, T *
 #undef KRON_GM
 }
 
-template <typename T, int PREC>
+// SIZED: dispatch modes with n_l, m_l <= 8 to compile-time-sized fibre
+// passes (fewer instructions per product, more registers: used by the
+// uneven-batch kernel, whose blocks are limited by shared memory anyway)
+template <typename T, int PREC, bool SIZED = false>
 __device__ void gen_apply_modes(const GenView &v, T *&cur, T *&nxt, const T *As, int C, int t,
                                 int GS, int g)
 {
@@ -524,7 +491,7 @@ __device__ void gen_apply_modes(const GenView &v, T *&cur, T *&nxt, const T *As,
       inner *= dims[u];
     const T *Aq         = As + aoff[q]; // Aq[i + j*mq]
     const long long tot = outer * mq * inner;
-    if (PREC != PREC_SPLIT && nq <= 8 && mq <= 8 && tot < (1LL << 31) &&
+    if (SIZED && PREC != PREC_SPLIT && nq <= 8 && mq <= 8 && tot < (1LL << 31) &&
         gen_mode_sized<T>(nq, mq, cur, nxt, Aq, (int)inner, (int)(outer * inner), t, GS))
     {
       // fibre per thread with compile-time sizes (done above)

@@ -110,7 +110,7 @@ __device__ __forceinline__ void vp_group_entry(const GenView &v, bool strided, c
     group_copy_tile(b0, x, rows_in, v.C, (int)v.total_cols, v.in_row, t, GS);
   group_sync(g, GS);
   double *cur = b0, *nxt = b1;
-  gen_apply_modes<double, PREC_F64>(v, cur, nxt, As, v.C, t, GS, g);
+  gen_apply_modes<double, PREC_F64, true>(v, cur, nxt, As, v.C, t, GS, g);
   if (!strided)
     group_flush(accum, out, cur, cur, false, rows_out, t, GS);
   else
