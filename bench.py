@@ -137,15 +137,27 @@ class XbatchedOverlap(Workload):
         self.pX = (self.dX.data_ptr() + 8 * self.L * torch.from_numpy(self.xlist)).to(dev)
         self.pY = (self.dY.data_ptr() + 8 * self.L * torch.from_numpy(self.ylist)).to(dev)
         self.seg = kb.Segments(self.pY) if mode == "segmented" else None
-        # e2e: pinned host copies of every input of the call
-        self.h = {k: v.cpu().pin_memory() for k, v in
-                  dict(A=self.dA, X=self.dX, Y=self.dY, pA=self.pA, pX=self.pX,
-                       pY=self.pY).items()}
+        # e2e: pinned host copies of every input of the call.  Atomic mode
+        # uploads the element grid as int32 index lists and builds the pointer
+        # arrays on the device (kron_build_pointers_async); segmented mode
+        # uploads the pointer arrays its plan was made for.
+        ilists = dict(alist=torch.from_numpy((self.a_offsets() // (self.n * self.n))
+                                             .astype(np.int32)),
+                      xlist=torch.from_numpy(self.xlist.astype(np.int32)),
+                      ylist=torch.from_numpy(self.ylist.astype(np.int32)))
+        host_in = dict(A=self.dA, X=self.dX, Y=self.dY)
+        if mode == "segmented":
+            host_in.update(pA=self.pA, pX=self.pX, pY=self.pY)
+        self.h = {k: v.cpu().pin_memory() for k, v in host_in.items()}
+        if mode != "segmented":
+            self.h.update({k: v.pin_memory() for k, v in ilists.items()})
+            self.dlist = {k: v.to(dev) for k, v in ilists.items()}
         self.hYout = torch.empty_like(self.h["Y"]).pin_memory()
         self.h2d_bytes = sum(v.numel() * v.element_size() for v in self.h.values())
         self.d2h_bytes = self.hYout.numel() * 8
         if mode != "segmented":
-            self.e2e_pipeline = (f"{E2E_CHUNKS} chunks of whole output elements; uploads, "
+            self.e2e_pipeline = (f"{E2E_CHUNKS} chunks of whole output elements; int32 index "
+                                 "lists up, pointer arrays built on the device; uploads, "
                                  "calls and downloads overlapped on 3 streams")
 
     def step(self):
@@ -159,8 +171,8 @@ class XbatchedOverlap(Workload):
         # host -> device (pinned, async), the library call(s), device -> host
         # of Y.  Atomic mode: entries are ordered by output element, so the
         # batch splits into chunks with disjoint Y ranges; X and the A pool
-        # go first, then per chunk its pointer arrays and Y columns, its call,
-        # and its Y columns back -- the same bytes, overlapped.
+        # go first, then per chunk its index lists and Y columns, the pointer
+        # build and the call, and its Y columns back -- overlapped.
         import torch
 
         h = self.h
@@ -177,13 +189,23 @@ class XbatchedOverlap(Workload):
         for c in range(E2E_CHUNKS):
             e0, e1 = c * E, (c + 1) * E if c < E2E_CHUNKS - 1 else self.batch
             y0, y1 = self.ylist[e0] * L, (self.ylist[e1 - 1] + 1) * L
-            h2d = [(self.pA[e0 * d:e1 * d], h["pA"][e0 * d:e1 * d]),
-                   (self.pX[e0:e1], h["pX"][e0:e1]), (self.pY[e0:e1], h["pY"][e0:e1]),
+            dl = self.dlist
+            h2d = [(dl["alist"][e0 * d:e1 * d], h["alist"][e0 * d:e1 * d]),
+                   (dl["xlist"][e0:e1], h["xlist"][e0:e1]), (dl["ylist"][e0:e1], h["ylist"][e0:e1]),
                    (self.dY[y0:y1], h["Y"][y0:y1])]
 
-            def run(s, e0=e0, e1=e1):
-                self.kb.kronmult_xbatched(d, self.n, self.pA[e0 * d:e1 * d], self.n,
-                                          self.pX[e0:e1], self.pY[e0:e1], stream=s)
+            def run(s, e0=e0, e1=e1, dl=dl):
+                pA = self.pA[e0 * d:e1 * d]
+                pX, pY = self.pX[e0:e1], self.pY[e0:e1]
+                nn = self.n * self.n
+                rc = self.kb.lib().kron_build_pointers_async(
+                    d, e1 - e0, self.dA.data_ptr(), nn, dl["alist"][e0 * d:e1 * d].data_ptr(),
+                    self.dX.data_ptr(), L, dl["xlist"][e0:e1].data_ptr(), self.dY.data_ptr(), L,
+                    dl["ylist"][e0:e1].data_ptr(), pA.data_ptr(), pX.data_ptr(), pY.data_ptr(),
+                    s.cuda_stream)
+                if rc != 0:
+                    raise RuntimeError(f"kron_build_pointers_async failed: {rc}")
+                self.kb.kronmult_xbatched(d, self.n, pA, self.n, pX, pY, stream=s)
 
             chunks.append((h2d, run, [(self.hYout[y0:y1], self.dY[y0:y1])]))
         self.run_pipeline(torch, [(self.dX, h["X"]), (self.dA, h["A"])], chunks)
