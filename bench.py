@@ -46,6 +46,12 @@ METRIC = "kronmult GFLOP/s + HBM GB/s vs roofline; FP32/split vs FP64 speedup at
 E2E_CHUNKS = 8
 
 
+def max_rel_err(torch, y, yref):
+    """max |y - yref| / max |yref| over the whole output (FP64)."""
+    den = yref.abs().max().item()
+    return (y.double() - yref).abs().max().item() / (den if den > 0 else 1.0)
+
+
 class Workload:
     name = ""
     dtype = "f64"
@@ -398,6 +404,71 @@ class UnevenBatch(Workload):
     def step(self):
         self.plan.execute(self.pA, self.pX, self.pY, self.dW)
 
+    def comparison(self, torch, timeit):
+        """The same entries as one plain kronmult{d}_vbatched call per
+        (d, shape) group, captured as one CUDA graph (and as host launches),
+        against the plan's persistent launches."""
+        import ctypes as C
+
+        kb = self.kb
+        lib = kb.lib()
+        dev = self.dA.device
+        self.dY.zero_()
+        self.step()
+        y_plan = self.dY.clone()
+        groups = {}
+        for k in range(self.batch):
+            d = int(self.shapes[k, 0])
+            groups.setdefault(tuple(int(v) for v in self.shapes[k, :1 + 2 * d]), []).append(k)
+        pa, px, py, glist = [], [], [], []
+        wmax = 0
+        for key, ks in sorted(groups.items()):
+            d = key[0]
+            m = (C.c_int * d)(*key[1::2])
+            n = (C.c_int * d)(*key[2::2])
+            wmax = max(wmax, lib.kron_vbatched_workspace_bytes(d, m, n, len(ks)))
+            glist.append((d, list(key[1:]), len(pa), len(px), len(ks)))
+            for k in ks:
+                pa.extend(int(self.a_off[6 * k + l]) for l in range(d))
+                px.append(int(self.x_off[k]))
+                py.append(int(self.y_off[k]))
+        gA = (self.dA.data_ptr() + 8 * torch.tensor(pa, dtype=torch.int64)).to(dev)
+        gX = (self.dX.data_ptr() + 8 * torch.tensor(px, dtype=torch.int64)).to(dev)
+        gY = (self.dY.data_ptr() + 8 * torch.tensor(py, dtype=torch.int64)).to(dev)
+        gW = torch.empty(max(1, wmax // 8), dtype=torch.float64, device=dev)
+        fns = {d: getattr(lib, f"kronmult{d}_vbatched_async") for d in range(1, 7)}
+
+        def run_groups():
+            st = torch.cuda.current_stream().cuda_stream
+            for d, mn, ia, ix, cnt in glist:
+                rc = fns[d](*mn, gA.data_ptr() + 8 * ia, gX.data_ptr() + 8 * ix,
+                            gY.data_ptr() + 8 * ix, gW.data_ptr(), wmax, cnt, st)
+                if rc != 0:
+                    raise RuntimeError(f"kronmult{d}_vbatched_async failed: {rc}")
+
+        ms_host = timeit(run_groups, reps=2)
+        graph = torch.cuda.CUDAGraph()
+        cs = torch.cuda.Stream()
+        cs.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(cs):
+            with torch.cuda.graph(graph, stream=cs):
+                run_groups()
+        torch.cuda.current_stream().wait_stream(cs)
+        ms_graph = timeit(graph.replay)
+        self.dY.zero_()
+        graph.replay()
+        torch.cuda.synchronize()
+        err = max_rel_err(torch, self.dY, y_plan)
+        del graph
+        flop = self.flops()
+        return {"per_group_calls": {
+            "groups": len(glist), "ms_per_step_graph": round(ms_graph, 4),
+            "value_graph": round(flop / ms_graph / 1e6, 2),
+            "ms_per_step_host_launches": round(ms_host, 4),
+            "value_host_launches": round(flop / ms_host / 1e6, 2), "unit": "GFLOP/s",
+            "max_rel_err_vs_plan": err,
+            "launch": "one kronmult{d}_vbatched call per (d, shape) group"}}
+
     def e2e_step(self):
         for k in ("A", "X", "Y", "pA", "pX", "pY"):
             getattr(self, "d" + k if k in ("A", "X", "Y") else k).copy_(self.h[k],
@@ -485,6 +556,55 @@ class XbatchedBig(Workload):
     def step(self):
         self.kb.kronmult_xbatched(self.d, self.n, self.pA, self.n, self.pX, self.pY, self.pW,
                                   subbatch=self.nw // 2)
+
+    def comparison(self, torch, timeit):
+        """The same xbatched call with the cluster kernel on CUDA-core FMAs
+        instead of the FP64 tensor cores (through the tuning table), and the
+        split hi+lo FP32 path against the FP64 path on the batched layout of
+        the same entries (split has no aliasing-output form)."""
+        kb, d, n, L, B = self.kb, self.d, self.n, self.L, self.batch
+        flop = self.flops()
+        out = {}
+        self.dY.zero_()
+        self.step()
+        y_tc = self.dY.clone()
+        kb.tune_set(d, n, "f64", "big", 2 | kb.BIG_CUDA_CORES)
+        try:
+            ms = timeit(self.step)
+            self.dY.zero_()
+            self.step()
+            torch.cuda.synchronize()
+            out["fp64_cuda_cores"] = {
+                "ms_per_step": round(ms, 4), "value": round(flop / ms / 1e6, 2),
+                "unit": "GFLOP/s", "max_rel_err_vs_fp64_tensor": max_rel_err(torch, self.dY, y_tc),
+                "kernel": "kron_big_kernel, 8x8 mode products as DFMA (no mma.sync)"}
+        finally:
+            kb.tune_set(d, n, "f64", None)
+        # batched layout: entry k's factors gathered from the pool, X as is,
+        # one output column per entry
+        aoff = torch.from_numpy(self.a_offsets()).to(self.dA.device)
+        Ab = (self.dA[aoff[:, None] + torch.arange(n * n, device=self.dA.device)]).reshape(-1)
+        Yb = torch.zeros(L * B, dtype=torch.float64, device=self.dA.device)
+        Wb = torch.empty(L * B, dtype=torch.float64, device=self.dA.device)
+        ms64 = timeit(lambda: kb.kronmult_batched(d, n, Ab, self.dX, Yb, Wb))
+        Yb.zero_()
+        kb.kronmult_batched(d, n, Ab, self.dX, Yb, Wb)
+        y64 = Yb.clone()
+        ms_sp = timeit(lambda: kb.kronmult_batched_split(d, n, Ab, self.dX, Yb, Wb))
+        Yb.zero_()
+        kb.kronmult_batched_split(d, n, Ab, self.dX, Yb, Wb)
+        torch.cuda.synchronize()
+        out["batched_fp64"] = {"ms_per_step": round(ms64, 4),
+                               "value": round(flop / ms64 / 1e6, 2), "unit": "GFLOP/s",
+                               "layout": f"batched, the same {B} entries, distinct outputs"}
+        out["batched_split"] = {
+            "ms_per_step": round(ms_sp, 4), "value": round(flop / ms_sp / 1e6, 2),
+            "unit": "GFLOP/s", "max_rel_err_vs_fp64": max_rel_err(torch, Yb, y64),
+            "arithmetic": "hi+lo FP32 parts of A and X, three cross products with compensated "
+                          "FP32 sums, CUDA cores (no TF32/BF16 tensor-core split)"}
+        del Ab, Yb, Wb, y_tc
+        torch.cuda.empty_cache()
+        return out
 
     def e2e_step(self):
         self.dA.copy_(self.h["A"], non_blocking=True)
@@ -781,6 +901,29 @@ def run_ours(args, world, rank, local):
 
     tot_ms, e2e_ms = max_over_ranks(dist, [tot_ms, e2e_ms], "cuda")
 
+    # comparison legs (rank 0, N=1 only; outside the timed region): other
+    # kernels on the same workload, each with its error against this run's
+    # FP64 result
+    comparison = None
+    if rank == 0 and world == 1 and not args.no_compare and hasattr(wl, "comparison"):
+        def timeit(fn, reps=3):
+            fn()
+            flush.zero_()
+            torch.cuda.synchronize()
+            evs = []
+            for _ in range(reps):
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record()
+                fn()
+                b.record()
+                flush.zero_()
+                evs.append((a, b))
+            torch.cuda.synchronize()
+            return sum(a.elapsed_time(b) for a, b in evs) / reps
+
+        comparison = wl.comparison(torch, timeit)
+
     # CPU baseline (rank 0, N=1 only): the reference's OpenMP build, bounded sample
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -838,6 +981,8 @@ def run_ours(args, world, rank, local):
                         "pipeline": wl.e2e_pipeline or "one call: uploads, call, download in order"},
                 "gpu_launches": args.steps * wl.launches_per_step,
                 "clocks": clocks}
+        if comparison:
+            line["comparison"] = comparison
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -888,6 +1033,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the comparison legs of configs 4 and 5")
     ap.add_argument("--autotune", action="store_true",
                     help="run the library's autotuner for the workload's shape first")
     ap.add_argument("--entries", type=int, default=0,

@@ -319,7 +319,9 @@ int kron_l2_persist_reset(kron_stream_t stream);
  *                       block (0: as many as fit)
  *   KRON_VARIANT_GEN    on-chip runtime-shape kernel
  *   KRON_VARIANT_BIG    cluster two-phase kernel; param = cluster size
- *                       (0: default)
+ *                       (0: default), plus KRON_BIG_CUDA_CORES to keep
+ *                       FP64 d = 6, n = 8 off the tensor cores (CUDA-core
+ *                       FMAs; other shapes ignore the bit)
  *   KRON_VARIANT_LARGE  two-phase launches through the workspace W
  * kron_autotune times every variant that runs (d, n, precision) on a
  * synthetic batched problem of up to batchCount entries (capped at 1 GiB),
@@ -343,6 +345,7 @@ int kron_l2_persist_reset(kron_stream_t stream);
 #define KRON_VARIANT_GEN 4
 #define KRON_VARIANT_BIG 5
 #define KRON_VARIANT_LARGE 6
+#define KRON_BIG_CUDA_CORES 256
 
 int kron_autotune(int d, int n, int precision, int batchCount, int *variant, int *param,
                   double *best_us, kron_stream_t stream);

@@ -235,6 +235,8 @@ def l2_persist_reset(stream=None):
 # ---------------------------------------------------------------- autotuner
 PRECISIONS = {"f64": 0, "f32": 1, "split": 2}
 VARIANTS = {1: "mma8", 2: "pipe", 3: "sq", 4: "gen", 5: "big", 6: "large"}
+# "big" param bit: FP64 d = 6, n = 8 on CUDA-core FMAs instead of tensor cores
+BIG_CUDA_CORES = 256
 
 
 def autotune(d, n, precision="f64", batch=1024, stream=None):

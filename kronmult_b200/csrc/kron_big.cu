@@ -23,6 +23,7 @@
 
 #include "kron_launch.h"
 #include "kron_mma8_core.cuh"
+#include "kronmult.h"
 
 namespace kron {
 
@@ -84,14 +85,16 @@ __device__ __forceinline__ T *big_slot(const BigWS &ws, int k, int e, int ebase,
                  : static_cast<T *>(ws.base) + (long long)(e - ebase) * ws.stride;
 }
 
-template <typename T, int D, int N, int Q, int C>
+// TC: FP64 n = 8 runs its 8x8 mode products on the tensor cores (mma.sync
+// f64); TC = false keeps every shape on CUDA-core FMAs (a comparison form)
+template <typename T, int D, int N, int Q, int C, bool TC = true>
 struct BigShape
 {
   static constexpr int LH   = cpow(N, Q);
   static constexpr int LT   = cpow(N, D - Q);
   static constexpr int L    = LH * LT;
   static constexpr int ASZ  = (D * N * N + 15) / 16 * 16;
-  static constexpr bool MMA = (sizeof(T) == 8) && (N == 8) && (D - Q == 3);
+  static constexpr bool MMA = TC && (sizeof(T) == 8) && (N == 8) && (D - Q == 3);
   // phase 1 without tensor cores: rounds of NB head rows share the block's
   // threads (LT/N fibres per row and mode)
   static constexpr int FPB  = LT / N;
@@ -99,7 +102,7 @@ struct BigShape
   static constexpr int RBUF = ((MMA ? 512 * BIG_WARPS : NB * LT) + 15) / 16 * 16;
   // phase 2 on FP64 tensor cores when the head is three 8x8 modes: tiles are
   // kept transposed, column c at c * PITCH (16-byte aligned columns)
-  static constexpr bool MMA2 = (sizeof(T) == 8) && (N == 8) && (Q == 3);
+  static constexpr bool MMA2 = TC && (sizeof(T) == 8) && (N == 8) && (Q == 3);
   static constexpr int PITCH = 514;
   static constexpr int TBUF  = ((MMA2 ? C * PITCH : LH * C) + 15) / 16 * 16;
   static constexpr size_t OFF_A    = 0;
@@ -192,11 +195,11 @@ __device__ __forceinline__ void tile_head_passes(T *tile, const T *As, int tid)
   }
 }
 
-template <typename T, int D, int N, int Q, int C, int MINB>
+template <typename T, int D, int N, int Q, int C, int MINB, bool TC>
 __global__ void __launch_bounds__(BIG_THREADS, MINB)
     kron_big_kernel(const __grid_constant__ Params p, const __grid_constant__ BigWS ws)
 {
-  using S            = BigShape<T, D, N, Q, C>;
+  using S            = BigShape<T, D, N, Q, C, TC>;
   constexpr int LH   = S::LH;
   constexpr int LT   = S::LT;
   constexpr int L    = S::L;
@@ -496,11 +499,11 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
   }
 }
 
-template <typename T, int D, int N, int Q, int C, int MINB>
+template <typename T, int D, int N, int Q, int C, int MINB, bool TC = true>
 int launch_big_t(Params p, const Workspace &wsp, int prec, int cluster, cudaStream_t stream)
 {
-  using S        = BigShape<T, D, N, Q, C>;
-  const void *fn = reinterpret_cast<const void *>(&kron_big_kernel<T, D, N, Q, C, MINB>);
+  using S        = BigShape<T, D, N, Q, C, TC>;
+  const void *fn = reinterpret_cast<const void *>(&kron_big_kernel<T, D, N, Q, C, MINB, TC>);
   if (S::SMEM > (size_t)device_info().max_smem_optin)
     return KRON_ERROR_NOT_SUPPORTED;
   int dummy = 1;
@@ -540,6 +543,7 @@ int launch_big_t(Params p, const Workspace &wsp, int prec, int cluster, cudaStre
 
   const long long work = p.eend - p.ebase;
   int cs               = 2;
+  cluster &= ~KRON_BIG_CUDA_CORES;
   if (cluster > 0)
     cs = std::min(8, cluster);
   else if (const char *env = std::getenv("KRON_BIG_CLUSTER"))
@@ -601,7 +605,9 @@ int launch_big(Params p, const Workspace &ws, int prec, int cluster, cudaStream_
   if (p.d == 6 && n == 7)
     return launch_big_t<double, 6, 7, 3, 8, 2>(p, ws, prec, cluster, stream);
   if (p.d == 6 && n == 8)
-    return launch_big_t<double, 6, 8, 3, 16, 1>(p, ws, prec, cluster, stream);
+    return (cluster & KRON_BIG_CUDA_CORES)
+               ? launch_big_t<double, 6, 8, 3, 16, 1, false>(p, ws, prec, cluster, stream)
+               : launch_big_t<double, 6, 8, 3, 16, 1>(p, ws, prec, cluster, stream);
   if (p.d == 5 && n == 8)
     return launch_big_t<double, 5, 8, 2, 32, 1>(p, ws, prec, cluster, stream);
   return KRON_ERROR_NOT_SUPPORTED;

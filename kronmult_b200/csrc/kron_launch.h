@@ -49,6 +49,7 @@ enum Variant : int
   VAR_SQ    = 3, // square on-chip kernel; param = entries per block (0: most that fit)
   VAR_GEN   = 4, // runtime-shape on-chip kernel (param unused)
   VAR_BIG   = 5, // cluster two-phase kernel; param = cluster size (0: default)
+                 // | KRON_BIG_CUDA_CORES (FP64 n = 8 without tensor cores)
   VAR_LARGE = 6, // two-phase launches through the workspace (param unused)
 };
 

@@ -191,7 +191,8 @@ extern "C" int kron_autotune(int d, int n, int precision, int batch, int *varian
   ws.wstride = L;
 
   // candidates: every variant, the square kernel at 1, 2, 4, ... entries
-  // per block, the cluster kernel at cluster sizes 1, 2, 4
+  // per block, the cluster kernel at cluster sizes 1, 2, 4 (FP64 n = 8: on
+  // the tensor cores and on CUDA cores)
   std::vector<std::pair<int, int>> cand = {{VAR_MMA8, 0}, {VAR_PIPE, 0}};
   const int ngmax = sq_entries_max(precision, d, n, false);
   for (int ng = 1; ng <= ngmax; ng *= 2)
@@ -200,7 +201,11 @@ extern "C" int kron_autotune(int d, int n, int precision, int batch, int *varian
     cand.push_back({VAR_SQ, ngmax});
   cand.push_back({VAR_GEN, 0});
   for (int cs : {1, 2, 4})
+  {
     cand.push_back({VAR_BIG, cs});
+    if (precision == PREC_F64 && d == 6 && n == 8)
+      cand.push_back({VAR_BIG, cs | KRON_BIG_CUDA_CORES});
+  }
   cand.push_back({VAR_LARGE, 0});
 
   cudaEvent_t e0, e1;

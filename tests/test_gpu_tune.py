@@ -64,6 +64,8 @@ def test_autotune_then_parity(gpu_lib, d, n, prec, batch):
     (5, 3, "f64", 90, "sq", 3), (5, 3, "f64", 90, "pipe", 0),
     (6, 6, "f64", 5, "big", 1), (6, 6, "f64", 5, "big", 2), (6, 6, "f64", 5, "big", 4),
     (6, 6, "f64", 5, "large", 0),
+    (6, 8, "f64", 3, "big", 2), (6, 8, "f64", 3, "big", 2 | kb.BIG_CUDA_CORES),
+    (6, 8, "f64", 3, "big", 1 | kb.BIG_CUDA_CORES),
     (6, 4, "f32", 70, "sq", 2), (6, 4, "f32", 70, "gen", 0),
     # a variant that cannot run the shape falls back to the built-in choice
     (4, 3, "f64", 50, "mma8", 0), (6, 6, "f64", 3, "pipe", 0),
