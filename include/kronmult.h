@@ -321,7 +321,11 @@ int kron_l2_persist_reset(kron_stream_t stream);
  *   KRON_VARIANT_BIG    cluster two-phase kernel; param = cluster size
  *                       (0: default), plus KRON_BIG_CUDA_CORES to keep
  *                       FP64 d = 6, n = 8 off the tensor cores (CUDA-core
- *                       FMAs; other shapes ignore the bit)
+ *                       FMAs; other shapes ignore the bit), plus
+ *                       KRON_BIG_SMEM_W to keep the intermediate in the
+ *                       cluster's shared memory instead of the workspace W
+ *                       (FP64 d = 6, n = 6; that form also runs, without
+ *                       the bit, when the caller passes no W)
  *   KRON_VARIANT_LARGE  two-phase launches through the workspace W
  * kron_autotune times every variant that runs (d, n, precision) on a
  * synthetic batched problem of up to batchCount entries (capped at 1 GiB),
@@ -346,6 +350,7 @@ int kron_l2_persist_reset(kron_stream_t stream);
 #define KRON_VARIANT_BIG 5
 #define KRON_VARIANT_LARGE 6
 #define KRON_BIG_CUDA_CORES 256
+#define KRON_BIG_SMEM_W 512
 
 int kron_autotune(int d, int n, int precision, int batchCount, int *variant, int *param,
                   double *best_us, kron_stream_t stream);

@@ -237,6 +237,9 @@ PRECISIONS = {"f64": 0, "f32": 1, "split": 2}
 VARIANTS = {1: "mma8", 2: "pipe", 3: "sq", 4: "gen", 5: "big", 6: "large"}
 # "big" param bit: FP64 d = 6, n = 8 on CUDA-core FMAs instead of tensor cores
 BIG_CUDA_CORES = 256
+# "big" param bit: keep the intermediate in the cluster's shared memory
+# instead of the workspace W (FP64 d = 6, n = 6)
+BIG_SMEM_W = 512
 
 
 def autotune(d, n, precision="f64", batch=1024, stream=None):

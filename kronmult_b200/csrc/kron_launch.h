@@ -50,6 +50,7 @@ enum Variant : int
   VAR_GEN   = 4, // runtime-shape on-chip kernel (param unused)
   VAR_BIG   = 5, // cluster two-phase kernel; param = cluster size (0: default)
                  // | KRON_BIG_CUDA_CORES (FP64 n = 8 without tensor cores)
+                 // | KRON_BIG_SMEM_W (FP64 n = 6: W in the cluster's shared memory)
   VAR_LARGE = 6, // two-phase launches through the workspace (param unused)
 };
 

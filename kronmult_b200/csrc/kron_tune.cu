@@ -192,7 +192,8 @@ extern "C" int kron_autotune(int d, int n, int precision, int batch, int *varian
 
   // candidates: every variant, the square kernel at 1, 2, 4, ... entries
   // per block, the cluster kernel at cluster sizes 1, 2, 4 (FP64 n = 8: on
-  // the tensor cores and on CUDA cores)
+  // the tensor cores and on CUDA cores; FP64 n = 6: W in the workspace or
+  // on chip)
   std::vector<std::pair<int, int>> cand = {{VAR_MMA8, 0}, {VAR_PIPE, 0}};
   const int ngmax = sq_entries_max(precision, d, n, false);
   for (int ng = 1; ng <= ngmax; ng *= 2)
@@ -200,6 +201,10 @@ extern "C" int kron_autotune(int d, int n, int precision, int batch, int *varian
   if (ngmax > 0 && (ngmax & (ngmax - 1)))
     cand.push_back({VAR_SQ, ngmax});
   cand.push_back({VAR_GEN, 0});
+  // FP64 d = 6, n = 6 can also keep W in the cluster's shared memory
+  // (fixed cluster of 2)
+  if (precision == PREC_F64 && d == 6 && n == 6)
+    cand.push_back({VAR_BIG, KRON_BIG_SMEM_W});
   for (int cs : {1, 2, 4})
   {
     cand.push_back({VAR_BIG, cs});

@@ -63,6 +63,7 @@ def test_autotune_then_parity(gpu_lib, d, n, prec, batch):
     (3, 8, "f64", 90, "mma8", 0), (3, 8, "f64", 90, "sq", 4), (3, 8, "f64", 90, "gen", 0),
     (5, 3, "f64", 90, "sq", 3), (5, 3, "f64", 90, "pipe", 0),
     (6, 6, "f64", 5, "big", 1), (6, 6, "f64", 5, "big", 2), (6, 6, "f64", 5, "big", 4),
+    (6, 6, "f64", 5, "big", kb.BIG_SMEM_W),
     (6, 6, "f64", 5, "large", 0),
     (6, 8, "f64", 3, "big", 2), (6, 8, "f64", 3, "big", 2 | kb.BIG_CUDA_CORES),
     (6, 8, "f64", 3, "big", 1 | kb.BIG_CUDA_CORES),
