@@ -154,7 +154,10 @@ def test_batched_vs_oracle(gpu_lib, d, n, batch):
 
 
 def test_batched_needs_workspace(gpu_lib):
-    d, n, batch = 6, 6, 2
+    """n^d beyond one block's shared memory and beyond a two-block cluster's
+    (d = 6, n = 7: 941 KB) needs the caller's W; d = 6, n = 6 no longer does
+    (W in the cluster's shared memory, tests/test_gpu_dsm.py)."""
+    d, n, batch = 6, 7, 2
     A, X, Y0 = _rand_batched(d, n, batch, 3)
     assert kb.lib().kron_batched_workspace_bytes(d, n, batch) > 0
     with pytest.raises(kb.KronError) as ei:
