@@ -69,7 +69,10 @@ const char *kron_version(void);
  * batched: A is (n,n,d,batchCount) contiguous; X, Y, W are (n^d, batchCount).
  * Replaces kronmult{d}_batched (kronmult6_batched.cpp:4-18).  Every entry
  * writes its own Y column.  W may be NULL when n^d doubles fit on chip
- * (kron_batched_workspace_bytes() returns 0 then).
+ * (kron_batched_workspace_bytes() returns 0 then), and for d = 6, n = 6,
+ * where a null W keeps the intermediate in a two-block cluster's shared
+ * memory (the query still returns the workspace form's need, the faster
+ * form when W is given).  The same holds for the pointer layouts.
  * ---------------------------------------------------------------------- */
 int kronmult1_batched_async(int n, double const Aarray_[], double Xarray_[], double Yarray_[],
                             double Warray_[], int batchCount, kron_stream_t stream);
