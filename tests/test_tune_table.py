@@ -42,6 +42,26 @@ def test_save_load_roundtrip(tmp_path):
     assert "6 6 0 5 4" in lines
 
 
+def test_cluster_kernel_form_bits_roundtrip(tmp_path):
+    """The "big" parameter carries the cluster size and the form bits (CUDA
+    cores for FP64 n = 8, the intermediate in shared memory for FP64 n = 6)
+    through the table and its file unchanged."""
+    import re
+
+    hdr = open(os.path.join(os.path.dirname(__file__), "..", "include", "kronmult.h")).read()
+    defs = dict(re.findall(r"#define (KRON_BIG_\w+) (\d+)", hdr))
+    assert int(defs["KRON_BIG_CUDA_CORES"]) == kb.BIG_CUDA_CORES
+    assert int(defs["KRON_BIG_SMEM_W"]) == kb.BIG_SMEM_W
+    kb.tune_set(6, 8, "f64", "big", 2 | kb.BIG_CUDA_CORES)
+    kb.tune_set(6, 6, "f64", "big", kb.BIG_SMEM_W)
+    path = os.path.join(tmp_path, "tune_bits.txt")
+    kb.tune_save(path)
+    kb.tune_clear()
+    kb.tune_load(path)
+    assert kb.tune_get(6, 8, "f64") == ("big", 2 | kb.BIG_CUDA_CORES)
+    assert kb.tune_get(6, 6, "f64") == ("big", kb.BIG_SMEM_W)
+
+
 @pytest.mark.parametrize("args", [
     (0, 4, 0, 3, 0), (7, 4, 0, 3, 0), (6, 0, 0, 3, 0), (6, 4, 3, 3, 0), (6, 4, 0, 9, 0),
     (6, 4, 0, 3, -1),
