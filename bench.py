@@ -2,18 +2,23 @@
 """Benchmark of the batched Kronecker matvec on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config 1..5] [--mode atomic|segmented]
+                    [--config 1..5] [--n N] [--precision f64|f32|split]
+                    [--mode atomic|segmented]
 
-Default workload (the overlapping-output case the headline metric is quoted
-on): kronmult3_xbatched, d=3, n=8, FP64; an element grid of 8192 elements,
-each coupled to itself and 15 distinct random neighbours -> 131072 entries,
-Ylist[k] = element i, Xlist[k] = element j; every A_l is a pointer into a
-pool of 64 random 8x8 matrices per dimension, N(0,1)/sqrt(8); X ~ U(-1,1).
-All data is synthetic (seeded numpy PCG64); the reference publishes no
-dataset.  Other --config values are measurement cases for the design notes
-(1: kronmult6_batched n=4 batch 512; 3: precision sweep n in {4,6} batch
-4096; 4: uneven batch of 20000 entries; 5: d=6 n=8 batch 1024 with shared
-outputs).
+Default workload (the headline): the precision sweep's largest case,
+kronmult6_batched with d=6, n=6, FP64, batchCount=4096 (46656-element
+vectors, 4.59 GB of algorithmic traffic per step), A ~ N(0,1)/sqrt(6),
+X ~ U(-1,1), Y from zero.  Its line also carries
+  - max_rel_err: the result of one step against the reference's own
+    OpenMP output on the same inputs, over the whole batch;
+  - comparison: FP32 and split (hi+lo FP32 arithmetic on FP64 data) legs at
+    n = 4 and n = 6 plus the FP64 leg at n = 4, each with its time, HBM GB/s
+    and error against the reference's FP64 output.
+Other --config values: 1 kronmult6_batched n=4 batch 512; 2 kronmult3_xbatched
+n=8 over 8192 elements x 16 couplings (131072 entries, overlapping outputs);
+3 the precision sweep (--n 4 or 6, --precision); 4 uneven batch of 20000
+entries; 5 d=6 n=8 batch 1024 with shared outputs.  All data is synthetic
+(seeded numpy PCG64); the reference publishes no dataset.
 
 One step = one call of the library over the whole batch with inputs resident
 in HBM.  Steps are timed one by one with CUDA events on the launching stream
@@ -52,11 +57,45 @@ def max_rel_err(torch, y, yref):
     return (y.double() - yref).abs().max().item() / (den if den > 0 else 1.0)
 
 
+def errors_vs(y, yref):
+    """Errors of a result against a reference output (host arrays): the
+    normwise relative error max |y - yref| / max |yref|, and the reference
+    tests' own measure, the largest absolute error max |y - yref|
+    (test_kronmult6_batched.cpp:393-394)."""
+    y = np.asarray(y, dtype=np.float64)
+    yref = np.asarray(yref, dtype=np.float64)
+    diff = float(np.abs(y - yref).max()) if y.size else 0.0
+    den = float(np.abs(yref).max()) if yref.size else 0.0
+    return {"max_rel_err": diff / (den if den > 0 else 1.0), "max_abs_err": diff}
+
+
 class Workload:
     name = ""
     dtype = "f64"
     launches_per_step = 1
     e2e_pipeline = None  # description of a chunked end-to-end step, if any
+    _yref = None
+
+    def reference_y(self):
+        """The reference's own output for the whole batch, Y from zero
+        (oracle/_ref: the reference's OpenMP build, recursive variant); cached."""
+        if self._yref is None:
+            import oracle
+
+            ref = oracle.Reference("recur")
+            self.cpu_setup(self.batch)
+            self.cpu_step(ref)
+            self._yref = self.cY.copy()
+        return self._yref
+
+    def check(self, torch, yref=None):
+        """Errors of one library step (Y from zero) against the reference's
+        output on the same inputs."""
+        yref = self.reference_y() if yref is None else yref
+        self.dY.zero_()
+        self.step()
+        torch.cuda.synchronize()
+        return errors_vs(self.dY.double().cpu().numpy(), yref)
 
     def flops(self) -> float:
         raise NotImplementedError
@@ -240,9 +279,11 @@ class XbatchedOverlap(Workload):
 class BatchedSquare(Workload):
     """kronmult{d}_batched (distinct outputs), FP64 / FP32 / split."""
 
-    def __init__(self, d=6, n=4, batch=512, precision="f64", dist="uniform", seed=SEED):
+    def __init__(self, d=6, n=4, batch=512, precision="f64", dist="uniform", seed=SEED,
+                 sweep=False):
         rng = np.random.default_rng(seed)
         self.d, self.n, self.batch, self.precision = d, n, batch, precision
+        self.dist, self.seed, self.sweep = dist, seed, sweep
         self.L = n ** d
         if dist == "uniform":
             self.A = rng.uniform(-1, 1, n * n * d * batch)
@@ -262,32 +303,88 @@ class BatchedSquare(Workload):
     def alg_bytes(self):
         return self.esize() * float(self.batch) * (3 * self.L + self.d * self.n * self.n)
 
-    def setup(self, torch, kb, mode):
+    def setup(self, torch, kb, mode, e2e=True):
         dev = torch.device("cuda")
         dt = torch.float32 if self.precision == "f32" else torch.float64
         self.kb = kb
         self.dA = torch.from_numpy(self.A).to(dev, dt)
         self.dX = torch.from_numpy(self.X).to(dev, dt)
         self.dY = torch.zeros(self.L * self.batch, dtype=dt, device=dev)
+        # the caller-owned W of the reference's contract, as large as the
+        # library's query asks
         need = kb.lib().kron_batched_workspace_bytes(self.d, self.n, self.batch)
         self.dW = torch.empty(max(1, need // 8), dtype=dt, device=dev) if need else None
-        # vectors beyond shared memory: one cluster-kernel launch for
-        # d=6 n=6..8 (FP64) / n=7..8 (FP32) and d=5 n=8 (FP64), else the
-        # two-phase path's two launches
+        # vectors beyond shared memory: one slab-cluster launch for d=6 n=6
+        # (FP64, FP32), one cluster two-phase launch for d=6 n=7..8 (FP64),
+        # n=7..8 (FP32) and d=5 n=8 (FP64), else the two-phase path's two
+        # launches
+        d, n, prec = self.d, self.n, self.precision
         if not need:
             self.launches_per_step = 1
+        elif d == 6 and n == 6 and prec in ("f64", "f32"):
+            self.launches_per_step = 1
         else:
-            d, n = self.d, self.n
-            fp64 = self.precision == "f64"
-            cluster = (d == 6 and (6 if fp64 else 7) <= n <= 8) or (fp64 and d == 5 and n == 8)
+            fp64 = prec == "f64"
+            cluster = (d == 6 and (6 if fp64 else 7) <= n <= 8 and prec != "split") or \
+                (fp64 and d == 5 and n == 8)
             self.launches_per_step = 1 if cluster else 2
+        self.e2e_pipeline = (f"{min(E2E_CHUNKS, self.batch)} chunks of entries; uploads, calls "
+                             "and downloads overlapped on 3 streams")
+        if not e2e:
+            return
         self.h = {k: v.cpu().pin_memory() for k, v in dict(A=self.dA, X=self.dX,
                                                           Y=self.dY).items()}
         self.hYout = torch.empty_like(self.h["Y"]).pin_memory()
         self.h2d_bytes = sum(v.numel() * v.element_size() for v in self.h.values())
         self.d2h_bytes = self.hYout.numel() * self.hYout.element_size()
-        self.e2e_pipeline = (f"{min(E2E_CHUNKS, self.batch)} chunks of entries; uploads, calls "
-                             "and downloads overlapped on 3 streams")
+
+    def release(self, torch):
+        for k in ("dA", "dX", "dY", "dW", "h", "hYout"):
+            if hasattr(self, k):
+                delattr(self, k)
+        torch.cuda.empty_cache()
+
+    def comparison(self, torch, timeit):
+        """The precision sweep (the headline's config): FP64, FP32 and split
+        (hi+lo FP32 arithmetic on FP64 data) at n = 4 and n = 6 on this
+        batch, each timed like the headline (mean of 3 steps, L2 flushed
+        between) and checked against the reference's FP64 output of the same
+        inputs; the headline's own case is timed again here for the speed-up
+        ratios."""
+        if not self.sweep:
+            return None
+        peaks, _ = read_peaks()
+        out = {}
+        for n in (4, 6):
+            yref = None
+            ms = {}
+            for prec in ("f64", "f32", "split"):
+                own = (n == self.n and prec == self.precision)
+                w = self if own else BatchedSquare(self.d, n, self.batch, prec, self.dist,
+                                                   self.seed)
+                if not own:
+                    w.setup(torch, self.kb, "atomic", e2e=False)
+                if yref is None:
+                    yref = w.reference_y()
+                t = timeit(w.step)
+                err = w.check(torch, yref)
+                gbs = w.alg_bytes() / t / 1e6
+                ms[prec] = t
+                out[f"n{n}_{prec}"] = {
+                    "ms_per_step": round(t, 4), "value": round(w.flops() / t / 1e6, 2),
+                    "unit": "GFLOP/s", "hbm_gbs": round(gbs, 1),
+                    "hbm_frac": round(gbs / peaks["hbm_gbs"], 4),
+                    "max_rel_err_vs_fp64_reference": err["max_rel_err"],
+                    "max_abs_err_vs_fp64_reference": err["max_abs_err"],
+                    "launches_per_step": w.launches_per_step}
+                if not own:
+                    w.release(torch)
+                    del w
+            out[f"n{n}_speedup_f32_over_f64"] = round(ms["f64"] / ms["f32"], 3)
+            out[f"n{n}_speedup_split_over_f64"] = round(ms["f64"] / ms["split"], 3)
+        out["reference_output"] = ("oracle/_ref (the reference's OpenMP build, recursive "
+                                   "variant) on the same inputs, whole batch, FP64")
+        return out
 
     def step(self):
         kb = self.kb
@@ -606,6 +703,26 @@ class XbatchedBig(Workload):
         torch.cuda.empty_cache()
         return out
 
+    def reference_y(self):
+        """The reference's kronmult6_xbatched over the whole batch on the
+        device's X (generated on the GPU), Y from zero; cached."""
+        if self._yref is None:
+            import oracle
+
+            ref = oracle.Reference("recur")
+            L, B = self.L, self.batch
+            X = self.dX.cpu().numpy()
+            Y = np.zeros(L * self.nout)
+            W = np.zeros(L * B)
+            ap = (self.Apool.ctypes.data + 8 * self.a_offsets()).astype(np.uint64)
+            xp = (X.ctypes.data + 8 * L * np.arange(B)).astype(np.uint64)
+            yp = (Y.ctypes.data + 8 * L * self.ylist).astype(np.uint64)
+            wp = (W.ctypes.data + 8 * L * np.arange(B)).astype(np.uint64)
+            ref.kronmult_xbatched(self.d, self.n, ap, self.n, xp, yp, wp, 0)
+            del W, X
+            self._yref = Y
+        return self._yref
+
     def e2e_step(self):
         self.dA.copy_(self.h["A"], non_blocking=True)
         self.dX.copy_(self.h["X"], non_blocking=True)
@@ -637,17 +754,16 @@ class XbatchedBig(Workload):
         return float(self.cs) * 2 * self.d * self.n ** (self.d + 1)
 
 
-def make_workload(cfg, precision, entries=0):
-    """The workload of --config cfg; entries > 0 scales its batch down (or
-    up) for small profiling cases (configs 1, 3 and 5; outputs of config 5
-    keep their 716:1024 ratio)."""
+def make_workload(cfg, precision, entries=0, n=6):
+    """The workload of --config cfg (n: config 3's size); entries > 0 scales
+    its batch down (or up) for small profiling cases (configs 1, 3 and 5;
+    outputs of config 5 keep their 716:1024 ratio)."""
     if cfg == 1:
         return BatchedSquare(6, 4, entries or 512, "f64", "uniform")
     if cfg == 2:
         return XbatchedOverlap()
     if cfg == 3:
-        n = int(os.environ.get("KRON_BENCH_N", "4"))
-        return BatchedSquare(6, n, entries or 4096, precision, "normal")
+        return BatchedSquare(6, n, entries or 4096, precision, "normal", sweep=not entries)
     if cfg == 4:
         return UnevenBatch()
     if cfg == 5:
@@ -668,17 +784,16 @@ def read_peaks():
 
 
 def profile_key(args):
-    """Key of a workload in the committed ncu summaries: `cfgN` for the
-    default precision, mode and size, with `-f32`, `-split`, `-segmented`,
-    `-nK` appended for the variants."""
+    """Key of a workload in the committed ncu summaries: `cfgN` for FP64,
+    atomic mode and the full batch (config 3 at n = 4), with `-f32`, `-split`,
+    `-segmented`, `-n6`, `-eK` appended for the variants."""
     key = f"cfg{args.config}"
     if args.precision != "f64":
         key += f"-{args.precision}"
     if args.mode != "atomic":
         key += f"-{args.mode}"
-    n = os.environ.get("KRON_BENCH_N")
-    if args.config == 3 and n and n != "4":
-        key += f"-n{n}"
+    if args.config == 3 and getattr(args, "n", 4) != 4:
+        key += f"-n{args.n}"
     if getattr(args, "entries", 0):
         key += f"-e{args.entries}"
     return key
@@ -772,7 +887,7 @@ def run_reference(args, world, rank):
         return
     import oracle
 
-    wl = make_workload(args.config, args.precision, args.entries)
+    wl = make_workload(args.config, args.precision, args.entries, args.n)
     if oracle.Reference.available("recur"):
         ref = oracle.Reference("recur")
         kind = "reference"
@@ -820,7 +935,7 @@ def run_ours(args, world, rank, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     kb.lib()
-    wl = make_workload(args.config, args.precision, args.entries)
+    wl = make_workload(args.config, args.precision, args.entries, args.n)
     tuned = None
     if args.autotune and hasattr(wl, "n") and hasattr(wl, "d"):
         # pick the kernel variant for this square (d, n, precision) before
@@ -901,9 +1016,22 @@ def run_ours(args, world, rank, local):
 
     tot_ms, e2e_ms = max_over_ranks(dist, [tot_ms, e2e_ms], "cuda")
 
+    # the stated error (rank 0, outside the timed region): one step from
+    # Y = 0 against the reference's own output on the same inputs
+    err = None
+    if rank == 0 and not args.no_check:
+        import oracle
+
+        if oracle.Reference.available("recur"):
+            err = wl.check(torch)
+            err["against"] = ("the reference's own output (oracle/_ref: its OpenMP build, "
+                              "recursive variant) on the same inputs, whole batch, FP64")
+        else:
+            err = {"unavailable": "oracle/_ref not built on this machine"}
+
     # comparison legs (rank 0, N=1 only; outside the timed region): other
-    # kernels on the same workload, each with its error against this run's
-    # FP64 result
+    # kernels on the same workload, each with its error against the FP64
+    # reference output
     comparison = None
     if rank == 0 and world == 1 and not args.no_compare and hasattr(wl, "comparison"):
         def timeit(fn, reps=3):
@@ -981,6 +1109,9 @@ def run_ours(args, world, rank, local):
                         "pipeline": wl.e2e_pipeline or "one call: uploads, call, download in order"},
                 "gpu_launches": args.steps * wl.launches_per_step,
                 "clocks": clocks}
+        if err is not None:
+            line["max_rel_err"] = err.get("max_rel_err")
+            line["err"] = err
         if comparison:
             line["comparison"] = comparison
         print(json.dumps(line), flush=True)
@@ -1026,7 +1157,9 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--config", type=int, default=3)
+    ap.add_argument("--n", type=int, default=int(os.environ.get("KRON_BENCH_N", "6")),
+                    choices=[4, 6], help="config 3: factor size (default 6)")
     ap.add_argument("--mode", default="atomic", choices=["atomic", "segmented"])
     ap.add_argument("--precision", default="f64", choices=["f64", "f32", "split"])
     ap.add_argument("--cpu-sample", type=int, default=1 << 30)
@@ -1034,7 +1167,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-compare", action="store_true",
-                    help="skip the comparison legs of configs 4 and 5")
+                    help="skip the comparison legs of configs 3, 4 and 5")
+    ap.add_argument("--no-check", action="store_true",
+                    help="skip the error check against the reference's output")
     ap.add_argument("--autotune", action="store_true",
                     help="run the library's autotuner for the workload's shape first")
     ap.add_argument("--entries", type=int, default=0,

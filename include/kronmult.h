@@ -216,9 +216,11 @@ int kronmult_batched_split_async(int d, int n, double const A[], double X[], dou
  * 16 MiB file-scope device array instead, which every GPU that loads the
  * library holds until exit.  n^d above 2,097,152 (16 MiB of doubles) is
  * rejected with KRON_ERROR_WORKSPACE.  Calls share that array: calls that
- * overlap on the GPU race; calls ordered on one stream are safe.  The first
- * call on a device looks the array's address up and should precede any
- * stream capture.  Allocates nothing.
+ * overlap on the GPU race; calls ordered on one stream are safe.  Every call
+ * outside stream capture looks the array's address up on the current device
+ * (any shape); a call under capture uses the address the last such lookup
+ * found, so the first call on a device should precede any stream capture.
+ * Allocates nothing.
  * ---------------------------------------------------------------------- */
 int kronmult_batched_noalloc_async(int d, int n, double const A[], double const X[], double Y[],
                                    int batchCount, kron_stream_t stream);
@@ -282,6 +284,24 @@ int kron_measure_fp64_peak(double *tensor_tflops, double *cuda_core_tflops);
  * clear != 0 resets the word.  Returns -1 if it cannot be read. */
 int kron_device_status(int clear);
 
+/* Bound on the polls of every asynchronous-copy wait in the kernels launched
+ * after this call (default 2^26; 0 restores the default).  A testing aid: a
+ * small bound makes a wait give up early -- the kernel then records 1 in the
+ * status word above, lets its copies land (always with the default bound),
+ * leaves y untouched for the entries it gave up on and returns -- so a test
+ * can drive the time-out path without a hung or faulted GPU.  Process-wide. */
+int kron_set_wait_limit(long long polls);
+
+/* Testing aid: the nth (0-based) device allocation the library makes after
+ * this call fails as if cudaMalloc had (-1: none; the default).  The calls
+ * that allocate -- kron_segments_create, kron_vplan_create, kron_autotune,
+ * kron_measure_fp64_peak -- then return KRON_ERROR_ALLOC with nothing left
+ * allocated.  Process-wide; the injection is used up by the failure. */
+int kron_test_fail_alloc(int nth);
+/* Testing aid: device allocations the library made and has not freed yet
+ * (plans alive, nothing else: every call frees its temporaries). */
+long long kron_test_live_allocs(void);
+
 /* ------------------------------------------------------------------------
  * Pointer arrays built on the device from integer lists (no reference
  * counterpart; the reference's tests build them on the host and copy them,
@@ -330,6 +350,9 @@ int kron_l2_persist_reset(kron_stream_t stream);
  *                       (FP64 d = 6, n = 6; that form also runs, without
  *                       the bit, when the caller passes no W)
  *   KRON_VARIANT_LARGE  two-phase launches through the workspace W
+ *   KRON_VARIANT_SLAB   slab-cluster kernel for d = 6, n = 6 (FP64 and
+ *                       FP32): one cluster of n blocks per entry, each block
+ *                       holding one n^5 slab, no workspace
  * kron_autotune times every variant that runs (d, n, precision) on a
  * synthetic batched problem of up to batchCount entries (capped at 1 GiB),
  * records the fastest for that key and returns it (outputs may be NULL).
@@ -352,6 +375,7 @@ int kron_l2_persist_reset(kron_stream_t stream);
 #define KRON_VARIANT_GEN 4
 #define KRON_VARIANT_BIG 5
 #define KRON_VARIANT_LARGE 6
+#define KRON_VARIANT_SLAB 7
 #define KRON_BIG_CUDA_CORES 256
 #define KRON_BIG_SMEM_W 512
 

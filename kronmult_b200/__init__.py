@@ -77,6 +77,9 @@ def _sig(lib):
     S["kron_version"] = []
     S["kron_measure_fp64_peak"] = [_vp, _vp]
     S["kron_device_status"] = [_i]
+    S["kron_set_wait_limit"] = [C.c_longlong]
+    S["kron_test_fail_alloc"] = [_i]
+    S["kron_test_live_allocs"] = []
     S["kron_build_pointers_async"] = [_i, _i, _vp, C.c_longlong, _vp, _vp, C.c_longlong, _vp,
                                       _vp, C.c_longlong, _vp, _vp, _vp, _vp, _vp]
     S["kron_l2_persist_async"] = [_vp, _sz, _vp]
@@ -99,6 +102,7 @@ def _sig(lib):
     lib.kron_status_string.restype = C.c_char_p
     lib.kron_version.restype = C.c_char_p
     lib.kron_tune_clear.restype = None
+    lib.kron_test_live_allocs.restype = C.c_longlong
     return lib
 
 
@@ -234,7 +238,7 @@ def l2_persist_reset(stream=None):
 
 # ---------------------------------------------------------------- autotuner
 PRECISIONS = {"f64": 0, "f32": 1, "split": 2}
-VARIANTS = {1: "mma8", 2: "pipe", 3: "sq", 4: "gen", 5: "big", 6: "large"}
+VARIANTS = {1: "mma8", 2: "pipe", 3: "sq", 4: "gen", 5: "big", 6: "large", 7: "slab"}
 # "big" param bit: FP64 d = 6, n = 8 on CUDA-core FMAs instead of tensor cores
 BIG_CUDA_CORES = 256
 # "big" param bit: keep the intermediate in the cluster's shared memory

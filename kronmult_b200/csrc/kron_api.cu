@@ -426,11 +426,11 @@ extern "C" int kron_segments_create(kron_segments_t *plan, double *const Yarray_
   pl->h_seg = seg;
   pl->d_perm = nullptr;
   pl->d_seg  = nullptr;
-  if (cudaMalloc(&pl->d_perm, sizeof(int) * std::max(1, batchCount)) != cudaSuccess ||
-      cudaMalloc(&pl->d_seg, sizeof(int) * seg.size()) != cudaSuccess)
+  if (kron::dev_malloc((void **)&pl->d_perm, sizeof(int) * std::max(1, batchCount)) != cudaSuccess ||
+      kron::dev_malloc((void **)&pl->d_seg, sizeof(int) * seg.size()) != cudaSuccess)
   {
-    cudaFree(pl->d_perm);
-    cudaFree(pl->d_seg);
+    kron::dev_free(pl->d_perm);
+    kron::dev_free(pl->d_seg);
     delete pl;
     return KRON_ERROR_ALLOC;
   }
@@ -440,8 +440,8 @@ extern "C" int kron_segments_create(kron_segments_t *plan, double *const Yarray_
       cudaMemcpy(pl->d_seg, seg.data(), sizeof(int) * seg.size(), cudaMemcpyHostToDevice) !=
           cudaSuccess)
   {
-    cudaFree(pl->d_perm);
-    cudaFree(pl->d_seg);
+    kron::dev_free(pl->d_perm);
+    kron::dev_free(pl->d_seg);
     delete pl;
     return KRON_ERROR_LAUNCH;
   }
@@ -453,8 +453,8 @@ extern "C" int kron_segments_destroy(kron_segments_t plan)
 {
   if (!plan)
     return KRON_SUCCESS;
-  cudaFree(plan->d_perm);
-  cudaFree(plan->d_seg);
+  kron::dev_free(plan->d_perm);
+  kron::dev_free(plan->d_seg);
   delete plan;
   return KRON_SUCCESS;
 }

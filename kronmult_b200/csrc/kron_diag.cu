@@ -73,7 +73,7 @@ extern "C" int kron_measure_fp64_peak(double *tensor_tflops, double *cuda_core_t
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return KRON_ERROR_LAUNCH;
   double *out = nullptr;
-  if (cudaMalloc(&out, 256 * sizeof(double)) != cudaSuccess)
+  if (kron::dev_malloc((void **)&out, 256 * sizeof(double)) != cudaSuccess)
     return KRON_ERROR_ALLOC;
   cudaEvent_t s = nullptr, e = nullptr;
   cudaEventCreate(&s);
@@ -103,7 +103,7 @@ extern "C" int kron_measure_fp64_peak(double *tensor_tflops, double *cuda_core_t
   cudaError_t err = cudaGetLastError();
   cudaEventDestroy(s);
   cudaEventDestroy(e);
-  cudaFree(out);
+  kron::dev_free(out);
   *tensor_tflops    = best_t;
   *cuda_core_tflops = best_c;
   return err == cudaSuccess ? KRON_SUCCESS : KRON_ERROR_LAUNCH;

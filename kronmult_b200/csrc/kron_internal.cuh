@@ -186,6 +186,11 @@ __device__ __forceinline__ void y_update(int accum, T *y, long long i, T v)
 
 // ---- host side ----------------------------------------------------------
 
+// cudaMalloc with the failure injection of kron_test_fail_alloc
+// (kron_status.cu); every device allocation of the library goes through it
+cudaError_t dev_malloc(void **ptr, size_t bytes);
+void dev_free(void *ptr);
+
 struct DeviceInfo
 {
   int device;

@@ -504,6 +504,8 @@ int launch_variant(Params p, int prec, const Workspace &ws, int variant, int par
   case VAR_BIG:
     return big_supported(p, prec) ? launch_big(p, ws, prec, param, stream)
                                   : KRON_ERROR_NOT_SUPPORTED;
+  case VAR_SLAB:
+    return slab_supported(p, prec) ? launch_slab(p, prec, stream) : KRON_ERROR_NOT_SUPPORTED;
   case VAR_LARGE:
     if (prec == PREC_F32)
       return launch_large_t<float>(prec, p, ws, stream);
@@ -531,11 +533,12 @@ int launch_kron(Params p, int prec, const Workspace &ws, cudaStream_t stream)
       return rc;
   }
   // default order: the specialised kernels, then the general ones
-  static const int order[] = {VAR_MMA8, VAR_PIPE, VAR_SQ, VAR_GEN, VAR_BIG, VAR_LARGE};
+  static const int order[] = {VAR_MMA8, VAR_PIPE, VAR_SLAB, VAR_SQ, VAR_GEN, VAR_BIG, VAR_LARGE};
   for (int v : order)
   {
     if ((v == VAR_MMA8 && std::getenv("KRON_DISABLE_MMA8")) ||
         (v == VAR_PIPE && std::getenv("KRON_DISABLE_PIPE")) ||
+        (v == VAR_SLAB && std::getenv("KRON_DISABLE_SLAB")) ||
         (v == VAR_BIG && std::getenv("KRON_DISABLE_BIG")))
       continue;
     const int rc = launch_variant(p, prec, ws, v, 0, stream);

@@ -25,9 +25,11 @@
 //   - every call shares the array, so calls whose work overlaps on the GPU
 //     (different streams without ordering, or different host threads) race
 //     and give wrong results; calls on one stream are ordered and safe;
-//   - the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress, once per device) and so should come before any
-//     stream capture.
+//   - every call looks up the array's device address (cudaGetSymbolAddress)
+//     on the current device, whatever the shape, so the address stays right
+//     after a context reset; while `stream` is capturing, the address that
+//     the last call outside capture found on this device is used instead.
+//     So the first call on a device should come before any stream capture.
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -47,18 +49,28 @@ std::mutex g_mu;
 void *g_scratch_addr[MAX_DEVICES] = {};
 
 // Device address of the scratch array for the current device (host code
-// must not use the symbol itself as a device pointer).
-int scratch_address(void **out)
+// must not use the symbol itself as a device pointer).  Looked up afresh
+// unless `stream` is capturing (a context reset may move the array); during
+// a capture the address cached by the last lookup on this device is used.
+int scratch_address(cudaStream_t stream, void **out)
 {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES)
     return KRON_ERROR_LAUNCH;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  // an error here (the legacy stream while another stream captures) counts
+  // as capturing
+  const bool capturing =
+      cudaStreamIsCapturing(stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone;
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_addr[dev])
+  if (!capturing || !g_scratch_addr[dev])
   {
     void *p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p)
+    {
+      cudaGetLastError();
       return KRON_ERROR_LAUNCH;
+    }
     g_scratch_addr[dev] = p;
   }
   *out = g_scratch_addr[dev];
@@ -104,21 +116,23 @@ extern "C" int kronmult_batched_noalloc_async(int d, int n, double const A[], do
   p.xstride = p.ystride = L;
   cudaStream_t s        = (cudaStream_t)stream;
 
+  // the address lookup comes first, whatever the shape, so that a first
+  // call with a small shape caches it for later calls under capture
+  void *scratch = nullptr;
+  int rc        = scratch_address(s, &scratch);
+  if (rc != KRON_SUCCESS)
+    return rc;
+
   if (fits_on_chip(d, p.m, p.n, PREC_F64, false))
   {
     p.ebase = 0;
     p.eend  = batchCount;
     Workspace ws{};
-    int rc = launch_kron(p, PREC_F64, ws, s);
+    rc = launch_kron(p, PREC_F64, ws, s);
     if (rc != KRON_SUCCESS)
       return rc;
     return cudaGetLastError() == cudaSuccess ? KRON_SUCCESS : KRON_ERROR_LAUNCH;
   }
-
-  void *scratch = nullptr;
-  int rc        = scratch_address(&scratch);
-  if (rc != KRON_SUCCESS)
-    return rc;
   // the batched two-phase path keeps entry k's intermediate at slot
   // (k - chunk start) * n^d
   const long long per_chunk = (long long)(KRON_NOALLOC_SCRATCH_BYTES / sizeof(double)) / L;

@@ -27,16 +27,16 @@
 // n = 4 the last two passes stay inside each warp's slabs and are separated
 // by a warp barrier only.
 //
-// Every mbarrier wait is bounded; on time-out the block records 1 in the
-// library's device status word (kron_device_status), lets the copies it
-// started land (bounded) and leaves.
+// Every mbarrier wait is bounded (wait_limit() polls); on time-out the block
+// records 1 in the library's device status word (kron_device_status), lets the
+// copies it started land (bounded by the full default limit, whatever the
+// wait limit) and leaves.
 #include <cstdint>
 
 #include "kron_launch.h"
+#include "kron_ptx.cuh"
 
 namespace kron {
-
-__device__ int g_device_status = 0;
 
 namespace {
 
@@ -48,7 +48,6 @@ namespace {
 
 constexpr int PIPE_THREADS = 256;
 constexpr int MAX_STAGES   = 6;
-constexpr long long SPIN_LIMIT = 1LL << 26;
 
 template <int N>
 struct GroupK
@@ -504,7 +503,8 @@ struct PipeOcc
 
 template <typename T, int D, int N>
 __global__ void __launch_bounds__(PIPE_THREADS, PipeOcc<T>::value)
-    kron_pipe_kernel(const __grid_constant__ Params p, int nstage)
+    kron_pipe_kernel(const __grid_constant__ Params p, int nstage, int *status, long long spin,
+                     long long drain)
 {
   using Lay = PipeLayout<T, D, N>;
   using P   = PipePlan<T, D, N>;
@@ -573,13 +573,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PipeOcc<T>::value)
     // wait for stage s (bounded); the outcome is combined at the barrier
     // below, after the A preparation (which reads in-bounds shared memory
     // either way)
-    bool done = false;
-    for (long long it = 0; it < SPIN_LIMIT; ++it)
-      if (mbar_try_wait(&bars[s], (phases >> s) & 1))
-      {
-        done = true;
-        break;
-      }
+    const bool done = ptx::mbar_wait_bounded(&bars[s], (phases >> s) & 1, spin);
     if (tid == 0 && done)
       inflight &= ~(1u << s);
     const int fl = meta[s];
@@ -618,11 +612,12 @@ __global__ void __launch_bounds__(PIPE_THREADS, PipeOcc<T>::value)
     {
       if (tid == 0)
       {
-        atomicExch(&g_device_status, 1);
+        if (status)
+          atomicExch(status, 1);
         // let the copies this block started land before it leaves (bounded)
         for (int s2 = 0; s2 < nstage; s2++)
           if ((inflight >> s2) & 1)
-            for (long long it = 0; it < SPIN_LIMIT; ++it)
+            for (long long it = 0; it < drain; ++it)
               if (mbar_try_wait(&bars[s2], (phases >> s2) & 1))
                 break;
         bulk_wait_all();
@@ -739,7 +734,10 @@ int launch_pipe_t(Params p, cudaStream_t stream)
   const long long work = p.eend - p.ebase;
   const long long grid =
       std::max<long long>(1, std::min<long long>(work, (long long)device_info().sms * per_sm));
-  void *args[]         = {&p, &ns};
+  int *status          = device_status_ptr();
+  long long spin       = wait_limit();
+  long long drain      = drain_limit();
+  void *args[]         = {&p, &ns, &status, &spin, &drain};
   return cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(PIPE_THREADS), args, smem, stream) ==
                  cudaSuccess
              ? KRON_SUCCESS
@@ -796,16 +794,3 @@ int launch_pipe(Params p, int prec, cudaStream_t stream)
 }
 
 } // namespace kron
-
-extern "C" int kron_device_status(int clear)
-{
-  int v = 0;
-  if (cudaMemcpyFromSymbol(&v, kron::g_device_status, sizeof(int)) != cudaSuccess)
-    return -1;
-  if (clear && v != 0)
-  {
-    int z = 0;
-    cudaMemcpyToSymbol(kron::g_device_status, &z, sizeof(int));
-  }
-  return v;
-}

@@ -1,0 +1,549 @@
+// Slab-cluster kernel: square d = 6 vectors too large for one block's shared
+// memory (n = 6: 373 KB per entry in FP64, 187 KB in FP32), with no
+// workspace and no intermediate traffic through L2 or HBM.
+//
+// One thread-block cluster of n blocks works on one entry at a time.  Block r
+// owns slab r of x, the n^5 contiguous elements with i_1 = r, brought into its
+// shared memory by one TMA bulk copy.  The six mode products run as three
+// register-blocked passes of two modes each.  Every thread takes one fibre of
+// n^2 elements per pass and holds one factor at a time in registers:
+//   pass A  modes 5, 6: fibres of n^2 contiguous slab elements;
+//   pass B  modes 3, 4: fibres (i_3, i_4) at slab strides n^3, n^2;
+//   pass C  modes 1, 2: block r takes the n^3 tuples t = (i_3..i_6) in
+//           [r n^3, (r+1) n^3) and reads the n^2 elements slab_{i_1}[i_2 n^4 +
+//           t] from the cluster's shared memory (ld.shared::cluster).
+// Pass C's results go to a staging buffer as n^2 rows (i_1, i_2) of n^3
+// contiguous elements, then into y by one TMA bulk reduce-add per row.  So y
+// is read and written once, in L2, and outputs that alias add up.
+//
+// Each block keeps two stages (x slab + factors), so the next entry's copies
+// land while this one computes.  The cluster barriers are split so that
+// independent work fills their latency:
+//
+//   arrive1(e) [pass A(e+1)] wait1(e)  pass C reads(e)  arrive2(e)
+//   [pass C math(e), staging + reduce-adds(e), pass B(e+1)]  wait2(e)
+//   refill the stage of e with entry e+2;  arrive1(e+1) ...
+//
+// Barrier 1 of entry e: every block has finished pass B(e), so pass C may
+// read.  Barrier 2 of entry e: every block has finished reading the others'
+// slabs of e, so the stage can be refilled and no block leaves while another
+// still reads it.
+//
+// Every mbarrier wait is bounded (wait_limit() polls).  A block whose copies
+// do not arrive in time does four things:
+//   - records 1 in the device status word;
+//   - marks itself dead in its shared memory;
+//   - stops issuing copies and reduce-adds;
+//   - before leaving, lets its outstanding copies land (bounded by
+//     drain_limit()).
+// The other blocks read the dead marks after barrier 1 and stop writing y
+// too.  All blocks still take every cluster barrier.
+//
+// The product is the reference's (kronmult6_batched.hpp:41-75, computed
+// there by kronmultv_recur.hpp:117-145): y += (A_1 x ... x A_6) x, with A_6's
+// index fastest.  The six mode products run in a different order, which
+// changes rounding only.
+#include <algorithm>
+#include <cstdint>
+
+#include "kron_launch.h"
+#include "kron_ptx.cuh"
+
+namespace kron {
+
+namespace {
+
+using namespace ptx;
+
+template <typename T, int N>
+struct SlabShape
+{
+  static constexpr int CS      = N; // blocks per cluster, one slab each
+  static constexpr int N2      = N * N;
+  static constexpr int N3      = N2 * N;
+  static constexpr int N4      = N3 * N;
+  static constexpr int N5      = N4 * N;
+  static constexpr int FIB     = N3; // fibres of every pass (pass C: tuples)
+  static constexpr int THREADS = (FIB + 31) / 32 * 32;
+  static constexpr int ASZ     = 6 * N2;
+  static constexpr size_t XB   = (size_t)N5 * sizeof(T);
+  static constexpr size_t AB   = ((size_t)ASZ * sizeof(T) + 15) / 16 * 16;
+  static constexpr size_t STAGE_BYTES = (XB + AB + 127) / 128 * 128;
+  // [0, 16) two mbarriers, [16, 20) dead mark, [20, 28) per-stage copy
+  // flags, [28, 32) dead mark of any block of the cluster
+  static constexpr size_t OFF_STAGE0 = 128;
+  static constexpr size_t OFF_OUT    = OFF_STAGE0 + 2 * STAGE_BYTES;
+  static constexpr size_t SMEM       = OFF_OUT + XB;
+  static constexpr int MINB          = (228 * 1024) / (int)(SMEM + 1024) > 0
+                                           ? (228 * 1024) / (int)(SMEM + 1024)
+                                           : 1;
+  // pass C's rows (n^3 elements at i_1 n^5 + i_2 n^4 + r n^3) are whole
+  // 16-byte units: bulk reduce-adds from the staging buffer
+  static constexpr bool ROWS16 = (N3 * sizeof(T)) % 16 == 0;
+  static constexpr bool XTMA   = XB % 16 == 0;
+  static_assert(N3 <= 1024, "one fibre per thread");
+};
+
+constexpr int FLAG_X_TMA = 1; // slab arrived by bulk copy
+constexpr int FLAG_A_TMA = 2; // A_1..A_6 arrived by bulk copy (contiguous)
+
+// factor A (column major, A(i, j) at i + j N) into registers
+template <typename T, int N>
+__device__ __forceinline__ void load_factor(const T *A, T (&a)[N][N])
+{
+#pragma unroll
+  for (int j = 0; j < N; j++)
+  {
+    if constexpr (sizeof(T) == 8 && N % 2 == 0)
+    {
+#pragma unroll
+      for (int i = 0; i < N; i += 2)
+      {
+        const double2 u = *reinterpret_cast<const double2 *>(A + i + j * N);
+        a[i][j]         = u.x;
+        a[i + 1][j]     = u.y;
+      }
+    }
+    else if constexpr (sizeof(T) == 4 && N % 2 == 0)
+    {
+#pragma unroll
+      for (int i = 0; i < N; i += 2)
+      {
+        const float2 u = *reinterpret_cast<const float2 *>(A + i + j * N);
+        a[i][j]        = u.x;
+        a[i + 1][j]    = u.y;
+      }
+    }
+    else
+    {
+#pragma unroll
+      for (int i = 0; i < N; i++)
+        a[i][j] = A[i + j * N];
+    }
+  }
+}
+
+// v is an n x n block, v[a N + b]: apply_fast applies A along b (the faster
+// mode), apply_slow along a
+template <typename T, int N>
+__device__ __forceinline__ void apply_fast(T (&v)[N * N], const T *A)
+{
+  T a[N][N];
+  load_factor<T, N>(A, a);
+#pragma unroll
+  for (int r = 0; r < N; r++)
+  {
+    T t[N];
+#pragma unroll
+    for (int i = 0; i < N; i++)
+    {
+      T z = a[i][0] * v[r * N];
+#pragma unroll
+      for (int j = 1; j < N; j++)
+        z = fma(a[i][j], v[r * N + j], z);
+      t[i] = z;
+    }
+#pragma unroll
+    for (int i = 0; i < N; i++)
+      v[r * N + i] = t[i];
+  }
+}
+
+template <typename T, int N>
+__device__ __forceinline__ void apply_slow(T (&v)[N * N], const T *A)
+{
+  T a[N][N];
+  load_factor<T, N>(A, a);
+#pragma unroll
+  for (int c = 0; c < N; c++)
+  {
+    T t[N];
+#pragma unroll
+    for (int i = 0; i < N; i++)
+    {
+      T z = a[i][0] * v[c];
+#pragma unroll
+      for (int j = 1; j < N; j++)
+        z = fma(a[i][j], v[j * N + c], z);
+      t[i] = z;
+    }
+#pragma unroll
+    for (int i = 0; i < N; i++)
+      v[i * N + c] = t[i];
+  }
+}
+
+// pass A: modes 5 (A_5, slow) and 6 (A_6, fast) on the contiguous fibre f
+template <typename T, int N>
+__device__ __forceinline__ void pass_a(T *slab, const T *As, int f)
+{
+  constexpr int N2 = N * N;
+  constexpr int V  = 16 / sizeof(T);
+  T *b             = slab + f * N2;
+  T v[N2];
+  if constexpr ((N2 * sizeof(T)) % 16 == 0)
+  {
+    // 16-byte aligned fibre: vector loads and stores
+#pragma unroll
+    for (int c = 0; c < N2; c += V)
+    {
+      if constexpr (sizeof(T) == 8)
+      {
+        const double2 u = *reinterpret_cast<const double2 *>(b + c);
+        v[c]            = u.x;
+        v[c + 1]        = u.y;
+      }
+      else
+      {
+        const float4 u = *reinterpret_cast<const float4 *>(b + c);
+        v[c]           = u.x;
+        v[c + 1]       = u.y;
+        v[c + 2]       = u.z;
+        v[c + 3]       = u.w;
+      }
+    }
+  }
+  else
+  {
+#pragma unroll
+    for (int c = 0; c < N2; c++)
+      v[c] = b[c];
+  }
+  apply_fast<T, N>(v, As + 5 * N2);
+  apply_slow<T, N>(v, As + 4 * N2);
+  if constexpr ((N2 * sizeof(T)) % 16 == 0)
+  {
+#pragma unroll
+    for (int c = 0; c < N2; c += V)
+    {
+      if constexpr (sizeof(T) == 8)
+        *reinterpret_cast<double2 *>(b + c) = make_double2(v[c], v[c + 1]);
+      else
+        *reinterpret_cast<float4 *>(b + c) = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+    }
+  }
+  else
+  {
+#pragma unroll
+    for (int c = 0; c < N2; c++)
+      b[c] = v[c];
+  }
+}
+
+// pass B: modes 3 (A_3, slow) and 4 (A_4, fast) on fibre f = (i_2, i_5, i_6)
+template <typename T, int N>
+__device__ __forceinline__ void pass_b(T *slab, const T *As, int f)
+{
+  constexpr int N2 = N * N, N3 = N2 * N, N4 = N3 * N;
+  const int o = f / N2, r = f - o * N2;
+  T *b        = slab + o * N4 + r;
+  T v[N2];
+#pragma unroll
+  for (int a = 0; a < N; a++)
+#pragma unroll
+    for (int c = 0; c < N; c++)
+      v[a * N + c] = b[a * N3 + c * N2];
+  apply_fast<T, N>(v, As + 3 * N2);
+  apply_slow<T, N>(v, As + 2 * N2);
+#pragma unroll
+  for (int a = 0; a < N; a++)
+#pragma unroll
+    for (int c = 0; c < N; c++)
+      b[a * N3 + c * N2] = v[a * N + c];
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(SlabShape<T, N>::THREADS, SlabShape<T, N>::MINB)
+    kron_slab_kernel(const __grid_constant__ Params p, int *status, long long spin,
+                     long long drain)
+{
+  using S            = SlabShape<T, N>;
+  constexpr int CS   = S::CS;
+  constexpr int N2   = S::N2, N3 = S::N3, N4 = S::N4, N5 = S::N5, ASZ = S::ASZ;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+  int *dead_mark = reinterpret_cast<int *>(smem + 16);
+  int *sflags    = reinterpret_cast<int *>(smem + 20);
+  int *peer_dead = reinterpret_cast<int *>(smem + 28);
+  T *obuf        = reinterpret_cast<T *>(smem + S::OFF_OUT);
+  auto stage_x   = [&](int s) {
+    return reinterpret_cast<T *>(smem + S::OFF_STAGE0 + s * S::STAGE_BYTES);
+  };
+  auto stage_a = [&](int s) {
+    return reinterpret_cast<T *>(smem + S::OFF_STAGE0 + s * S::STAGE_BYTES + S::XB);
+  };
+  const int tid  = threadIdx.x;
+  const int rank = (int)cluster_ctarank();
+  const int cid  = blockIdx.x / CS;
+  const int ncl  = gridDim.x / CS;
+  const long long tot = p.eend - p.ebase;
+  const int eb = p.ebase + (int)(tot * cid / ncl);
+  const int ee = p.ebase + (int)(tot * (cid + 1) / ncl);
+  if (eb >= ee)
+    return; // the whole cluster leaves together
+
+  if (tid == 0)
+  {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    *dead_mark = 0;
+    *peer_dead = 0;
+    fence_mbar_init();
+  }
+  __syncthreads();
+  // every block of the cluster is running before any shared::cluster access
+  cluster_sync();
+
+  unsigned inflight = 0; // thread 0: stages whose copies were not waited for
+  unsigned phase    = 0; // bit s: parity of stage s's next completion
+  bool dead         = false;
+
+  // thread 0: start the copies of position e into stage s
+  auto issue = [&](int e, int s) {
+    EntryRef<T> en;
+    entry_fetch<T>(p, entry_index(p, e), 6, en);
+    const T *xs      = en.x + (long long)rank * N5;
+    const bool x_tma = S::XTMA && aligned16(xs);
+    const bool a_tma = (p.layout == LAYOUT_BATCHED || p.layout == LAYOUT_PBATCHED) &&
+                       (ASZ * sizeof(T)) % 16 == 0 && aligned16(en.A[0]);
+    sflags[s] = (x_tma ? FLAG_X_TMA : 0) | (a_tma ? FLAG_A_TMA : 0);
+    const unsigned bytes =
+        (x_tma ? (unsigned)S::XB : 0u) + (a_tma ? (unsigned)(ASZ * sizeof(T)) : 0u);
+    fence_proxy_async();
+    mbar_expect_tx(&bars[s], bytes);
+    if (x_tma)
+      tma_load_1d(stage_x(s), xs, (unsigned)S::XB, &bars[s]);
+    if (a_tma)
+      tma_load_1d(stage_a(s), en.A[0], (unsigned)(ASZ * sizeof(T)), &bars[s]);
+    inflight |= 1u << s;
+  };
+
+  // every thread: wait for stage s (position e) and load what its copies did
+  // not carry; a time-out makes the block dead
+  auto acquire = [&](int e, int s) {
+    bool ok = true;
+    if (!dead)
+    {
+      ok = mbar_wait_bounded(&bars[s], (phase >> s) & 1, spin);
+      if (ok)
+      {
+        phase ^= 1u << s;
+        if (tid == 0)
+          inflight &= ~(1u << s);
+        const int fl = sflags[s];
+        if ((fl & (FLAG_X_TMA | FLAG_A_TMA)) != (FLAG_X_TMA | FLAG_A_TMA))
+        {
+          EntryRef<T> en;
+          entry_fetch<T>(p, entry_index(p, e), 6, en);
+          if (!(fl & FLAG_X_TMA))
+          {
+            const T *xs = en.x + (long long)rank * N5;
+            T *sx       = stage_x(s);
+            for (int i = tid; i < N5; i += blockDim.x)
+              sx[i] = xs[i];
+          }
+          if (!(fl & FLAG_A_TMA))
+          {
+            T *sa = stage_a(s);
+            for (int q = tid; q < ASZ; q += blockDim.x)
+            {
+              const int l = q / N2, ij = q - l * N2;
+              const int j = ij / N, i = ij - j * N;
+              sa[q]       = en.A[l][i + (long long)j * en.ld[l]];
+            }
+          }
+        }
+      }
+    }
+    if (!__syncthreads_and(ok) && !dead)
+    {
+      dead = true;
+      if (tid == 0)
+      {
+        if (status)
+          atomicExch(status, 1);
+        *dead_mark = 1;
+      }
+    }
+  };
+
+  if (tid == 0)
+  {
+    issue(eb, 0);
+    if (eb + 1 < ee)
+      issue(eb + 1, 1);
+  }
+
+  // passes A and B of the first position
+  acquire(eb, 0);
+  if (tid < N3)
+    pass_a<T, N>(stage_x(0), stage_a(0), tid);
+  __syncthreads();
+  if (tid < N3)
+    pass_b<T, N>(stage_x(0), stage_a(0), tid);
+  cluster_arrive(); // barrier 1 (eb)
+
+  const unsigned dead_addr = smem_addr(dead_mark);
+  for (int e = eb; e < ee; ++e)
+  {
+    const int s     = (e - eb) & 1;
+    const bool more = e + 1 < ee;
+    // pass A of the next position while barrier 1 settles
+    if (more)
+    {
+      acquire(e + 1, s ^ 1);
+      if (tid < N3)
+        pass_a<T, N>(stage_x(s ^ 1), stage_a(s ^ 1), tid);
+    }
+    cluster_wait(); // barrier 1 (e): every block finished pass B(e)
+    if (tid == 0)
+    {
+      int any = 0;
+#pragma unroll
+      for (int a = 0; a < CS; a++)
+        any |= ld_cluster_s32(mapa(dead_addr, (unsigned)a));
+      *peer_dead = any;
+    }
+    // pass C: tuple t of every slab of the cluster
+    T v[N2];
+    const unsigned sbase = smem_addr(stage_x(s));
+    const int t          = rank * N3 + tid;
+    if (tid < N3)
+    {
+#pragma unroll
+      for (int a = 0; a < CS; a++)
+      {
+        const unsigned base = mapa(sbase, (unsigned)a);
+#pragma unroll
+        for (int c = 0; c < N; c++)
+          v[a * N + c] = ld_cluster<T>(base + (unsigned)((c * N4 + t) * sizeof(T)));
+      }
+    }
+    // this thread's generic accesses to stage s come before the refill's
+    // bulk copy into it
+    fence_proxy_async();
+    cluster_arrive(); // barrier 2 (e): this block's reads of the slabs are done
+    if (tid < N3)
+    {
+      apply_fast<T, N>(v, stage_a(s) + 1 * N2);
+      apply_slow<T, N>(v, stage_a(s) + 0 * N2);
+    }
+    T *y            = entry_y<T>(p, entry_index(p, e)) + (long long)rank * N3;
+    const bool bulk = S::ROWS16 && aligned16(y);
+    if (tid == 0)
+      bulk_wait_read(); // the previous position's rows have left the staging buffer
+    __syncthreads();
+    dead = dead || (*peer_dead != 0);
+    if (!dead)
+    {
+      if (bulk)
+      {
+        if (tid < N3)
+#pragma unroll
+          for (int q = 0; q < N2; q++)
+            obuf[q * N3 + tid] = v[q];
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0)
+        {
+#pragma unroll 1
+          for (int q = 0; q < N2; q++)
+          {
+            const int a = q / N, c = q - a * N;
+            bulk_reduce_add<T>(y + (long long)a * N5 + (long long)c * N4, obuf + q * N3,
+                               (unsigned)(N3 * sizeof(T)));
+          }
+          bulk_commit();
+        }
+      }
+      else if (tid < N3)
+      {
+#pragma unroll
+        for (int q = 0; q < N2; q++)
+        {
+          const int a = q / N, c = q - a * N;
+          atomicAdd(y + (long long)a * N5 + (long long)c * N4 + tid, v[q]);
+        }
+      }
+    }
+    if (more && tid < N3)
+      pass_b<T, N>(stage_x(s ^ 1), stage_a(s ^ 1), tid);
+    cluster_wait(); // barrier 2 (e): no block reads this block's stage s any more
+    if (tid == 0 && !dead && e + 2 < ee)
+      issue(e + 2, s);
+    if (more)
+      cluster_arrive(); // barrier 1 (e+1)
+  }
+
+  if (tid == 0)
+  {
+    if (dead)
+      for (int s = 0; s < 2; s++)
+        if ((inflight >> s) & 1)
+          mbar_wait_bounded(&bars[s], (phase >> s) & 1, drain);
+    bulk_wait_all();
+  }
+}
+
+template <typename T, int N>
+int launch_slab_t(Params p, cudaStream_t stream)
+{
+  using S        = SlabShape<T, N>;
+  const void *fn = reinterpret_cast<const void *>(&kron_slab_kernel<T, N>);
+  if (S::SMEM > (size_t)device_info().max_smem_optin)
+    return KRON_ERROR_NOT_SUPPORTED;
+  int per_sm = 1;
+  if (cached_occupancy(fn, S::THREADS, S::SMEM, &per_sm) != KRON_SUCCESS)
+    return KRON_ERROR_LAUNCH;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id               = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = S::CS;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim             = dim3(S::THREADS);
+  cfg.dynamicSmemBytes     = S::SMEM;
+  cfg.stream               = stream;
+  cfg.attrs                = attr;
+  cfg.numAttrs             = 1;
+  cfg.gridDim              = dim3((device_info().sms / S::CS) * S::CS);
+  int ncl                  = 0;
+  if (cudaOccupancyMaxActiveClusters(&ncl, fn, &cfg) != cudaSuccess || ncl < 1)
+  {
+    cudaGetLastError();
+    return KRON_ERROR_NOT_SUPPORTED;
+  }
+  ncl          = (int)std::min<long long>((long long)ncl, p.eend - p.ebase);
+  cfg.gridDim  = dim3(ncl * S::CS);
+  int *status  = device_status_ptr();
+  long long sp = wait_limit();
+  long long dr = drain_limit();
+  void *args[] = {&p, &status, &sp, &dr};
+  return cudaLaunchKernelExC(&cfg, fn, args) == cudaSuccess ? KRON_SUCCESS : KRON_ERROR_LAUNCH;
+}
+
+} // namespace
+
+bool slab_supported(const Params &p, int prec)
+{
+  if ((prec != PREC_F64 && prec != PREC_F32) || p.seg_off ||
+      (p.accum != ACC_DISTINCT && p.accum != ACC_ATOMIC) || p.d != 6)
+    return false;
+  const int n = p.n[0];
+  for (int l = 0; l < p.d; l++)
+    if (p.m[l] != n || p.n[l] != n)
+      return false;
+  return n == 6;
+}
+
+int launch_slab(Params p, int prec, cudaStream_t stream)
+{
+  if (p.eend <= p.ebase)
+    return KRON_SUCCESS;
+  if (p.n[0] == 6)
+    return prec == PREC_F32 ? launch_slab_t<float, 6>(p, stream)
+                            : launch_slab_t<double, 6>(p, stream);
+  return KRON_ERROR_NOT_SUPPORTED;
+}
+
+} // namespace kron

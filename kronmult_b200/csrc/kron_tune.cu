@@ -42,7 +42,7 @@ struct TuneChoice
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneChoice> g_tune;
 
-bool valid_variant(int v) { return v >= VAR_MMA8 && v <= VAR_LARGE; }
+bool valid_variant(int v) { return v >= VAR_MMA8 && v <= VAR_SLAB; }
 
 } // namespace
 
@@ -68,7 +68,8 @@ static_assert(KRON_PREC_F64 == PREC_F64 && KRON_PREC_F32 == PREC_F32 &&
               "precision codes");
 static_assert(KRON_VARIANT_MMA8 == VAR_MMA8 && KRON_VARIANT_PIPE == VAR_PIPE &&
                   KRON_VARIANT_SQ == VAR_SQ && KRON_VARIANT_GEN == VAR_GEN &&
-                  KRON_VARIANT_BIG == VAR_BIG && KRON_VARIANT_LARGE == VAR_LARGE,
+                  KRON_VARIANT_BIG == VAR_BIG && KRON_VARIANT_LARGE == VAR_LARGE &&
+                  KRON_VARIANT_SLAB == VAR_SLAB,
               "variant codes");
 
 extern "C" int kron_tune_set(int d, int n, int precision, int variant, int param)
@@ -139,9 +140,9 @@ struct DevBuf
   ~DevBuf()
   {
     if (p)
-      cudaFree(p);
+      kron::dev_free(p);
   }
-  bool alloc(size_t bytes) { return bytes == 0 || cudaMalloc(&p, bytes) == cudaSuccess; }
+  bool alloc(size_t bytes) { return bytes == 0 || dev_malloc(&p, bytes) == cudaSuccess; }
 };
 
 } // namespace
@@ -194,7 +195,7 @@ extern "C" int kron_autotune(int d, int n, int precision, int batch, int *varian
   // per block, the cluster kernel at cluster sizes 1, 2, 4 (FP64 n = 8: on
   // the tensor cores and on CUDA cores; FP64 n = 6: W in the workspace or
   // on chip)
-  std::vector<std::pair<int, int>> cand = {{VAR_MMA8, 0}, {VAR_PIPE, 0}};
+  std::vector<std::pair<int, int>> cand = {{VAR_MMA8, 0}, {VAR_PIPE, 0}, {VAR_SLAB, 0}};
   const int ngmax = sq_entries_max(precision, d, n, false);
   for (int ng = 1; ng <= ngmax; ng *= 2)
     cand.push_back({VAR_SQ, ng});
@@ -213,9 +214,13 @@ extern "C" int kron_autotune(int d, int n, int precision, int batch, int *varian
   }
   cand.push_back({VAR_LARGE, 0});
 
-  cudaEvent_t e0, e1;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+  {
+    if (e0)
+      cudaEventDestroy(e0);
     return KRON_ERROR_ALLOC;
+  }
   int best_v = 0, best_p = 0;
   float best = 0.f;
   for (const auto &c : cand)

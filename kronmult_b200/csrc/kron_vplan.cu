@@ -536,13 +536,13 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
   pl->d_desc      = nullptr;
   pl->d_items     = nullptr;
   pl->d_counters  = nullptr;
-  if (cudaMalloc(&pl->d_counters, 8 * sizeof(int)) != cudaSuccess ||
-      (batchCount > 0 && cudaMalloc(&pl->d_desc, sizeof(VDesc) * batchCount) != cudaSuccess) ||
-      (!items.empty() && cudaMalloc(&pl->d_items, sizeof(VItem) * items.size()) != cudaSuccess))
+  if (kron::dev_malloc((void **)&pl->d_counters, 8 * sizeof(int)) != cudaSuccess ||
+      (batchCount > 0 && kron::dev_malloc((void **)&pl->d_desc, sizeof(VDesc) * batchCount) != cudaSuccess) ||
+      (!items.empty() && kron::dev_malloc((void **)&pl->d_items, sizeof(VItem) * items.size()) != cudaSuccess))
   {
-    cudaFree(pl->d_items);
-    cudaFree(pl->d_desc);
-    cudaFree(pl->d_counters);
+    kron::dev_free(pl->d_items);
+    kron::dev_free(pl->d_desc);
+    kron::dev_free(pl->d_counters);
     delete pl;
     return KRON_ERROR_ALLOC;
   }
@@ -551,9 +551,9 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
       (!items.empty() && cudaMemcpy(pl->d_items, items.data(), sizeof(VItem) * items.size(),
                                     cudaMemcpyHostToDevice) != cudaSuccess))
   {
-    cudaFree(pl->d_items);
-    cudaFree(pl->d_desc);
-    cudaFree(pl->d_counters);
+    kron::dev_free(pl->d_items);
+    kron::dev_free(pl->d_desc);
+    kron::dev_free(pl->d_counters);
     delete pl;
     return KRON_ERROR_LAUNCH;
   }
@@ -567,9 +567,9 @@ extern "C" int kron_vplan_destroy(kron_vplan_t plan)
     return KRON_SUCCESS;
   if (plan->exec)
     cudaGraphExecDestroy(plan->exec);
-  cudaFree(plan->d_items);
-  cudaFree(plan->d_desc);
-  cudaFree(plan->d_counters);
+  kron::dev_free(plan->d_items);
+  kron::dev_free(plan->d_desc);
+  kron::dev_free(plan->d_counters);
   delete plan;
   return KRON_SUCCESS;
 }

@@ -8,22 +8,19 @@ import pytest
 import bench
 
 
-def _args(config, precision="f64", mode="atomic", entries=0):
-    return argparse.Namespace(config=config, precision=precision, mode=mode, entries=entries)
+def _args(config, precision="f64", mode="atomic", entries=0, n=6):
+    return argparse.Namespace(config=config, precision=precision, mode=mode, entries=entries,
+                              n=n)
 
 
 @pytest.mark.parametrize("config,precision,n,key", [
-    (1, "f64", None, "cfg1"), (2, "f64", None, "cfg2"), (3, "f64", None, "cfg3"),
-    (3, "f32", None, "cfg3-f32"), (3, "split", None, "cfg3-split"),
-    (3, "f64", "6", "cfg3-n6"), (3, "f32", "6", "cfg3-f32-n6"),
-    (4, "f64", None, "cfg4"), (5, "f64", None, "cfg5"),
+    (1, "f64", 6, "cfg1"), (2, "f64", 6, "cfg2"), (3, "f64", 4, "cfg3"),
+    (3, "f32", 4, "cfg3-f32"), (3, "split", 4, "cfg3-split"),
+    (3, "f64", 6, "cfg3-n6"), (3, "f32", 6, "cfg3-f32-n6"),
+    (4, "f64", 6, "cfg4"), (5, "f64", 6, "cfg5"),
 ])
-def test_every_workload_has_a_traffic_line(monkeypatch, config, precision, n, key):
-    if n is None:
-        monkeypatch.delenv("KRON_BENCH_N", raising=False)
-    else:
-        monkeypatch.setenv("KRON_BENCH_N", n)
-    args = _args(config, precision)
+def test_every_workload_has_a_traffic_line(config, precision, n, key):
+    args = _args(config, precision, n=n)
     assert bench.profile_key(args) == key
     traffic, src = bench.read_profile_traffic(key)
     assert traffic is not None and traffic > 0, key
