@@ -17,7 +17,8 @@ X ~ U(-1,1), Y from zero.  Its line also carries
 Other --config values: 1 kronmult6_batched n=4 batch 512; 2 kronmult3_xbatched
 n=8 over 8192 elements x 16 couplings (131072 entries, overlapping outputs);
 3 the precision sweep (--n 4 or 6, --precision); 4 uneven batch of 20000
-entries; 5 d=6 n=8 batch 1024 with shared outputs.  All data is synthetic
+entries; 5 d=6 n=8 batch 1024 with shared outputs; 6 kgemm_nn_batched
+64x64x64, batch 32768.  All data is synthetic
 (seeded numpy PCG64); the reference publishes no dataset.
 
 One step = one call of the library over the whole batch with inputs resident
@@ -380,11 +381,43 @@ class BatchedSquare(Workload):
                 if not own:
                     w.release(torch)
                     del w
+                if n == 4 and prec == "f64":
+                    out["n4_repeated_apply"] = self._repeated_apply(torch, w)
             out[f"n{n}_speedup_f32_over_f64"] = round(ms["f64"] / ms["f32"], 3)
             out[f"n{n}_speedup_split_over_f64"] = round(ms["f64"] / ms["split"], 3)
         out["reference_output"] = ("oracle/_ref (the reference's OpenMP build, recursive "
                                    "variant) on the same inputs, whole batch, FP64")
         return out
+
+    def _repeated_apply(self, torch, w, reps=50):
+        """A solver's repeated apply: the same factors A applied `reps` times
+        back to back (no L2 flush between), without and then with A kept in
+        L2 by kron_l2_persist_async; mean microseconds per apply."""
+        kb = self.kb
+        res = {}
+        for persist in (False, True):
+            if persist:
+                kb.l2_persist(w.dA)
+            try:
+                w.step()
+                torch.cuda.synchronize()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record()
+                for _ in range(reps):
+                    w.step()
+                b.record()
+                torch.cuda.synchronize()
+                res["us_per_apply_l2_persist" if persist else "us_per_apply"] = round(
+                    1e3 * a.elapsed_time(b) / reps, 2)
+            finally:
+                if persist:
+                    kb.l2_persist_reset()
+        res["a_bytes"] = int(w.dA.numel() * w.dA.element_size())
+        res["apply_bytes"] = w.alg_bytes()
+        res["note"] = (f"{reps} applies of the same A back to back; the window keeps A "
+                       "(the fixed operand) in L2 while X and Y stream")
+        return res
 
     def step(self):
         kb = self.kb
@@ -754,6 +787,78 @@ class XbatchedBig(Workload):
         return float(self.cs) * 2 * self.d * self.n ** (self.d + 1)
 
 
+class KgemmBatched(Workload):
+    """kgemm_nn_batched, the reference's batched small GEMM: mm = nn = kk =
+    64 (the largest size its tests sweep, test_kgemm_nn_batched.cpp:491-533),
+    C_k += A_k B_k (alpha = 1, beta = 1: the accumulate form the Kronecker
+    kernels call), distinct C_k, A/B/C ~ U(-1,1)."""
+
+    def __init__(self, batch=32768, mm=64, nn=64, kk=64, seed=SEED + 6):
+        rng = np.random.default_rng(seed)
+        self.batch, self.mm, self.nn, self.kk = batch, mm, nn, kk
+        self.A = rng.uniform(-1, 1, mm * kk * batch)
+        self.B = rng.uniform(-1, 1, kk * nn * batch)
+        self.C0 = rng.uniform(-1, 1, mm * nn * batch)
+        self.name = f"kgemm_nn_batched {mm}x{nn}x{kk}, batch {batch}, alpha=1 beta=1, FP64"
+
+    def flops(self):
+        return 2.0 * self.mm * self.nn * self.kk * self.batch
+
+    def alg_bytes(self):
+        return 8.0 * self.batch * (self.mm * self.kk + self.kk * self.nn + 2 * self.mm * self.nn)
+
+    def _ptrs(self, torch, base, stride):
+        return (base.data_ptr() + 8 * stride * torch.arange(self.batch, dtype=torch.int64)).to(
+            base.device)
+
+    def setup(self, torch, kb, mode):
+        dev = torch.device("cuda")
+        self.kb = kb
+        self.dA = torch.from_numpy(self.A).to(dev)
+        self.dB = torch.from_numpy(self.B).to(dev)
+        self.dY = torch.from_numpy(self.C0).to(dev)
+        mm, nn, kk = self.mm, self.nn, self.kk
+        self.pA = self._ptrs(torch, self.dA, mm * kk)
+        self.pB = self._ptrs(torch, self.dB, kk * nn)
+        self.pC = self._ptrs(torch, self.dY, mm * nn)
+        self.ldA = torch.full((self.batch,), mm, dtype=torch.int32, device=dev)
+        self.ldB = torch.full((self.batch,), kk, dtype=torch.int32, device=dev)
+        self.ldC = torch.full((self.batch,), mm, dtype=torch.int32, device=dev)
+        self.h = {k: v.cpu().pin_memory() for k, v in dict(A=self.dA, B=self.dB,
+                                                          C=self.dY).items()}
+        self.hYout = torch.empty_like(self.h["C"]).pin_memory()
+        self.h2d_bytes = sum(v.numel() * v.element_size() for v in self.h.values())
+        self.d2h_bytes = self.hYout.numel() * 8
+
+    def step(self):
+        self.kb.kgemm_batched("nn", self.mm, self.nn, self.kk, 1.0, self.pA, self.ldA, self.pB,
+                              self.ldB, 1.0, self.pC, self.ldC)
+
+    def e2e_step(self):
+        self.dA.copy_(self.h["A"], non_blocking=True)
+        self.dB.copy_(self.h["B"], non_blocking=True)
+        self.dY.copy_(self.h["C"], non_blocking=True)
+        self.step()
+        self.hYout.copy_(self.dY, non_blocking=True)
+
+    def cpu_setup(self, sample_entries):
+        self.cs = min(self.batch, sample_entries)
+        mm, nn, kk, cs = self.mm, self.nn, self.kk, self.cs
+        self.cY = np.zeros(mm * nn * cs)
+        self.c_ap = (self.A.ctypes.data + 8 * mm * kk * np.arange(cs)).astype(np.uint64)
+        self.c_bp = (self.B.ctypes.data + 8 * kk * nn * np.arange(cs)).astype(np.uint64)
+        self.c_cp = (self.cY.ctypes.data + 8 * mm * nn * np.arange(cs)).astype(np.uint64)
+        self.c_ld = [np.full(cs, v, dtype=np.int32) for v in (mm, kk, mm)]
+        return cs
+
+    def cpu_step(self, ref):
+        ref.kgemm_batched("nn", self.mm, self.nn, self.kk, 1.0, self.c_ap, self.c_ld[0],
+                          self.c_bp, self.c_ld[1], 1.0, self.c_cp, self.c_ld[2])
+
+    def cpu_flops(self):
+        return 2.0 * self.mm * self.nn * self.kk * self.cs
+
+
 def make_workload(cfg, precision, entries=0, n=6):
     """The workload of --config cfg (n: config 3's size); entries > 0 scales
     its batch down (or up) for small profiling cases (configs 1, 3 and 5;
@@ -770,6 +875,8 @@ def make_workload(cfg, precision, entries=0, n=6):
         if entries:
             return XbatchedBig(batch=entries, nout=max(1, entries * 716 // 1024))
         return XbatchedBig()
+    if cfg == 6:
+        return KgemmBatched(batch=entries or 32768)
     raise SystemExit(f"--config {cfg} not available in this bench")
 
 

@@ -505,7 +505,8 @@ int launch_variant(Params p, int prec, const Workspace &ws, int variant, int par
     return big_supported(p, prec) ? launch_big(p, ws, prec, param, stream)
                                   : KRON_ERROR_NOT_SUPPORTED;
   case VAR_SLAB:
-    return slab_supported(p, prec) ? launch_slab(p, prec, stream) : KRON_ERROR_NOT_SUPPORTED;
+    return slab_supported(p, prec) ? launch_slab(p, prec, param, stream)
+                                    : KRON_ERROR_NOT_SUPPORTED;
   case VAR_LARGE:
     if (prec == PREC_F32)
       return launch_large_t<float>(prec, p, ws, stream);

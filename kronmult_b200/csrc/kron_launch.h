@@ -37,7 +37,7 @@ int launch_pipe(Params p, int prec, cudaStream_t stream);
 // Slab-cluster kernel for square d = 6 vectors beyond one block's shared
 // memory whose n slabs of n^5 elements fit (kron_slab.cu).
 bool slab_supported(const Params &p, int prec);
-int launch_slab(Params p, int prec, cudaStream_t stream);
+int launch_slab(Params p, int prec, int flags, cudaStream_t stream);
 
 // Device status word (kron_status.cu): its device address for kernel
 // arguments, the poll bound of mbarrier waits (kron_set_wait_limit), and the
@@ -64,7 +64,7 @@ enum Variant : int
                  // | KRON_BIG_CUDA_CORES (FP64 n = 8 without tensor cores)
                  // | KRON_BIG_SMEM_W (FP64 n = 6: W in the cluster's shared memory)
   VAR_LARGE = 6, // two-phase launches through the workspace (param unused)
-  VAR_SLAB  = 7, // slab-cluster kernel, no workspace (param unused)
+  VAR_SLAB  = 7, // slab-cluster kernel, no workspace; param: KRON_SLAB_NO_ROTATE
 };
 
 // Work items of a launch (launch_kron does this before any variant).

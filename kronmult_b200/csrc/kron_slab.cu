@@ -150,10 +150,25 @@ __device__ __forceinline__ void apply_fast(T (&v)[N * N], const T *A)
 }
 
 template <typename T, int N>
-__device__ __forceinline__ void apply_slow(T (&v)[N * N], const T *A)
+__device__ __forceinline__ void apply_slow(T (&v)[N * N], const T *A, int rot = 0)
 {
   T a[N][N];
-  load_factor<T, N>(A, a);
+  if (rot == 0)
+    load_factor<T, N>(A, a);
+  else
+  {
+    // rows of v hold rows (r + rot) mod N: the factor with rows and columns
+    // rotated the same way gives the rotated rows of the product
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+      for (int j = 0; j < N; j++)
+      {
+        const int ri = i + rot < N ? i + rot : i + rot - N;
+        const int rj = j + rot < N ? j + rot : j + rot - N;
+        a[i][j]      = A[ri + rj * N];
+      }
+  }
 #pragma unroll
   for (int c = 0; c < N; c++)
   {
@@ -173,13 +188,20 @@ __device__ __forceinline__ void apply_slow(T (&v)[N * N], const T *A)
   }
 }
 
-// pass A: modes 5 (A_5, slow) and 6 (A_6, fast) on the contiguous fibre f
+// pass A: modes 5 (A_5, slow) and 6 (A_6, fast) on the contiguous fibre f.
+// FP64 fibres of n^2 = 36 elements start 18 16-byte units apart, so lanes f
+// and f + 4 of a quarter-warp would hit the same banks on every vector
+// access; with `rotate`, lanes with bit 2 set walk their rows starting one
+// row later (a 3-unit shift, which makes the eight lanes' units distinct)
+// and apply A_5 with rotated indices.
 template <typename T, int N>
-__device__ __forceinline__ void pass_a(T *slab, const T *As, int f)
+__device__ __forceinline__ void pass_a(T *slab, const T *As, int f, bool rotate)
 {
   constexpr int N2 = N * N;
   constexpr int V  = 16 / sizeof(T);
   T *b             = slab + f * N2;
+  // rotation by whole rows keeps the 16-byte units inside rows
+  const int rot = (sizeof(T) == 8 && N % 2 == 0 && rotate) ? ((f >> 2) & 1) : 0;
   T v[N2];
   if constexpr ((N2 * sizeof(T)) % 16 == 0)
   {
@@ -189,7 +211,9 @@ __device__ __forceinline__ void pass_a(T *slab, const T *As, int f)
     {
       if constexpr (sizeof(T) == 8)
       {
-        const double2 u = *reinterpret_cast<const double2 *>(b + c);
+        int src = c + rot * N;
+        src     = src < N2 ? src : src - N2;
+        const double2 u = *reinterpret_cast<const double2 *>(b + src);
         v[c]            = u.x;
         v[c + 1]        = u.y;
       }
@@ -210,14 +234,18 @@ __device__ __forceinline__ void pass_a(T *slab, const T *As, int f)
       v[c] = b[c];
   }
   apply_fast<T, N>(v, As + 5 * N2);
-  apply_slow<T, N>(v, As + 4 * N2);
+  apply_slow<T, N>(v, As + 4 * N2, rot);
   if constexpr ((N2 * sizeof(T)) % 16 == 0)
   {
 #pragma unroll
     for (int c = 0; c < N2; c += V)
     {
       if constexpr (sizeof(T) == 8)
-        *reinterpret_cast<double2 *>(b + c) = make_double2(v[c], v[c + 1]);
+      {
+        int dst = c + rot * N;
+        dst     = dst < N2 ? dst : dst - N2;
+        *reinterpret_cast<double2 *>(b + dst) = make_double2(v[c], v[c + 1]);
+      }
       else
         *reinterpret_cast<float4 *>(b + c) = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
     }
@@ -255,7 +283,7 @@ __device__ __forceinline__ void pass_b(T *slab, const T *As, int f)
 template <typename T, int N>
 __global__ void __launch_bounds__(SlabShape<T, N>::THREADS, SlabShape<T, N>::MINB)
     kron_slab_kernel(const __grid_constant__ Params p, int *status, long long spin,
-                     long long drain)
+                     long long drain, int flags)
 {
   using S            = SlabShape<T, N>;
   constexpr int CS   = S::CS;
@@ -272,8 +300,9 @@ __global__ void __launch_bounds__(SlabShape<T, N>::THREADS, SlabShape<T, N>::MIN
   auto stage_a = [&](int s) {
     return reinterpret_cast<T *>(smem + S::OFF_STAGE0 + s * S::STAGE_BYTES + S::XB);
   };
-  const int tid  = threadIdx.x;
-  const int rank = (int)cluster_ctarank();
+  const int tid     = threadIdx.x;
+  const int rank    = (int)cluster_ctarank();
+  const bool rotate = !(flags & KRON_SLAB_NO_ROTATE);
   const int cid  = blockIdx.x / CS;
   const int ncl  = gridDim.x / CS;
   const long long tot = p.eend - p.ebase;
@@ -377,7 +406,7 @@ __global__ void __launch_bounds__(SlabShape<T, N>::THREADS, SlabShape<T, N>::MIN
   // passes A and B of the first position
   acquire(eb, 0);
   if (tid < N3)
-    pass_a<T, N>(stage_x(0), stage_a(0), tid);
+    pass_a<T, N>(stage_x(0), stage_a(0), tid, rotate);
   __syncthreads();
   if (tid < N3)
     pass_b<T, N>(stage_x(0), stage_a(0), tid);
@@ -393,7 +422,7 @@ __global__ void __launch_bounds__(SlabShape<T, N>::THREADS, SlabShape<T, N>::MIN
     {
       acquire(e + 1, s ^ 1);
       if (tid < N3)
-        pass_a<T, N>(stage_x(s ^ 1), stage_a(s ^ 1), tid);
+        pass_a<T, N>(stage_x(s ^ 1), stage_a(s ^ 1), tid, rotate);
     }
     cluster_wait(); // barrier 1 (e): every block finished pass B(e)
     if (tid == 0)
@@ -486,7 +515,7 @@ __global__ void __launch_bounds__(SlabShape<T, N>::THREADS, SlabShape<T, N>::MIN
 }
 
 template <typename T, int N>
-int launch_slab_t(Params p, cudaStream_t stream)
+int launch_slab_t(Params p, int flags, cudaStream_t stream)
 {
   using S        = SlabShape<T, N>;
   const void *fn = reinterpret_cast<const void *>(&kron_slab_kernel<T, N>);
@@ -518,7 +547,7 @@ int launch_slab_t(Params p, cudaStream_t stream)
   int *status  = device_status_ptr();
   long long sp = wait_limit();
   long long dr = drain_limit();
-  void *args[] = {&p, &status, &sp, &dr};
+  void *args[] = {&p, &status, &sp, &dr, &flags};
   return cudaLaunchKernelExC(&cfg, fn, args) == cudaSuccess ? KRON_SUCCESS : KRON_ERROR_LAUNCH;
 }
 
@@ -536,13 +565,13 @@ bool slab_supported(const Params &p, int prec)
   return n == 6;
 }
 
-int launch_slab(Params p, int prec, cudaStream_t stream)
+int launch_slab(Params p, int prec, int flags, cudaStream_t stream)
 {
   if (p.eend <= p.ebase)
     return KRON_SUCCESS;
   if (p.n[0] == 6)
-    return prec == PREC_F32 ? launch_slab_t<float, 6>(p, stream)
-                            : launch_slab_t<double, 6>(p, stream);
+    return prec == PREC_F32 ? launch_slab_t<float, 6>(p, flags, stream)
+                            : launch_slab_t<double, 6>(p, flags, stream);
   return KRON_ERROR_NOT_SUPPORTED;
 }
 

@@ -44,12 +44,14 @@ def _inputs(batch, seed, ny=None):
 
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 @pytest.mark.parametrize("batch", [1, 7, 40, 150])
-@pytest.mark.parametrize("forced", [False, True])
+@pytest.mark.parametrize("forced", [None, 0, kb.SLAB_NO_ROTATE])
 def test_slab_batched(gpu_lib, prec, batch, forced):
+    """forced: None = built-in choice, else the slab variant with that param
+    (with and without the lane rotation of its first pass)."""
     import torch
 
-    if forced:
-        kb.tune_set(D, N, prec, "slab", 0)
+    if forced is not None:
+        kb.tune_set(D, N, prec, "slab", forced)
     A, X, Y0 = _inputs(batch, 600 + batch)
     Yref = Y0.copy()
     oracle.kronmult_batched(D, N, A, X, Yref)
