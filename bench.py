@@ -378,11 +378,11 @@ class BatchedSquare(Workload):
                     "max_rel_err_vs_fp64_reference": err["max_rel_err"],
                     "max_abs_err_vs_fp64_reference": err["max_abs_err"],
                     "launches_per_step": w.launches_per_step}
+                if n == 4 and prec == "f64":
+                    out["n4_repeated_apply"] = self._repeated_apply(torch, w)
                 if not own:
                     w.release(torch)
                     del w
-                if n == 4 and prec == "f64":
-                    out["n4_repeated_apply"] = self._repeated_apply(torch, w)
             out[f"n{n}_speedup_f32_over_f64"] = round(ms["f64"] / ms["f32"], 3)
             out[f"n{n}_speedup_split_over_f64"] = round(ms["f64"] / ms["split"], 3)
         out["reference_output"] = ("oracle/_ref (the reference's OpenMP build, recursive "
