@@ -12,22 +12,25 @@
 //   pass C  modes 1, 2: block r takes the n^3 tuples t = (i_3..i_6) in
 //           [r n^3, (r+1) n^3) and reads the n^2 elements slab_{i_1}[i_2 n^4 +
 //           t] from the cluster's shared memory (ld.shared::cluster).
-// Pass C's results go to a staging buffer as n^2 rows (i_1, i_2) of n^3
-// contiguous elements, then into y by one TMA bulk reduce-add per row.  So y
-// is read and written once, in L2, and outputs that alias add up.
+// Once every block has read the slabs, pass C's results go over the block's
+// own slab as n^2 rows (i_1, i_2) of n^3 contiguous elements, and into y by
+// one TMA bulk reduce-add per row.  So y is read and written once, in L2, and
+// outputs that alias add up.
 //
-// Each block keeps two stages (x slab + factors), so the next entry's copies
-// land while this one computes.  The cluster barriers are split so that
-// independent work fills their latency:
+// Each block keeps a ring of three stages (x slab + factors): the entry being
+// computed, the next one (already landed), and the one after it, whose copy
+// is issued at the start of an iteration into the stage the previous entry
+// just left, so every copy has a whole iteration to land.  The cluster
+// barriers are split so that independent work fills their latency:
 //
-//   arrive1(e) [pass A(e+1)] wait1(e)  pass C reads(e)  arrive2(e)
-//   [pass C math(e), staging + reduce-adds(e), pass B(e+1)]  wait2(e)
-//   refill the stage of e with entry e+2;  arrive1(e+1) ...
+//   [pass A(e+1), refill stage(e-1) with e+2]  wait1(e)  pass C reads(e)
+//   arrive2(e)  [pass C math(e), pass B(e+1)]  wait2(e)
+//   results(e) over stage(e), bulk reduce-adds;  arrive1(e+1) ...
 //
 // Barrier 1 of entry e: every block has finished pass B(e), so pass C may
 // read.  Barrier 2 of entry e: every block has finished reading the others'
-// slabs of e, so the stage can be refilled and no block leaves while another
-// still reads it.
+// slabs of e, so the slab can take the results, the stage can be refilled
+// later, and no block leaves while another still reads it.
 //
 // Every mbarrier wait is bounded (wait_limit() polls).  A block whose copies
 // do not arrive in time does four things:
@@ -69,14 +72,23 @@ struct SlabShape
   static constexpr size_t XB   = (size_t)N5 * sizeof(T);
   static constexpr size_t AB   = ((size_t)ASZ * sizeof(T) + 15) / 16 * 16;
   static constexpr size_t STAGE_BYTES = (XB + AB + 127) / 128 * 128;
-  // [0, 16) two mbarriers, [16, 20) dead mark, [20, 28) per-stage copy
-  // flags, [28, 32) dead mark of any block of the cluster
-  static constexpr size_t OFF_STAGE0 = 128;
-  static constexpr size_t OFF_OUT    = OFF_STAGE0 + 2 * STAGE_BYTES;
-  static constexpr size_t SMEM       = OFF_OUT + XB;
-  static constexpr int MINB          = (228 * 1024) / (int)(SMEM + 1024) > 0
-                                           ? (228 * 1024) / (int)(SMEM + 1024)
-                                           : 1;
+  static constexpr int NS      = 3; // stages: computing, landing, being refilled
+  // header: NS mbarriers, this block's dead mark, the cluster's dead mark,
+  // per-stage copy flags
+  static constexpr size_t OFF_BARS      = 0;
+  static constexpr size_t OFF_DEAD      = 8 * NS;
+  static constexpr size_t OFF_PEER_DEAD = OFF_DEAD + 4;
+  static constexpr size_t OFF_FLAGS     = OFF_PEER_DEAD + 4;
+  static constexpr size_t OFF_STAGE0    = 128;
+  static constexpr size_t SMEM          = OFF_STAGE0 + NS * STAGE_BYTES;
+  static_assert(OFF_FLAGS + 4 * NS <= OFF_STAGE0, "header");
+  // blocks per SM that the shared memory allows, and the register cap that
+  // lets that many blocks of THREADS threads share the 64K registers
+  static constexpr int MINB   = (228 * 1024) / (int)(SMEM + 1024) > 0
+                                    ? (228 * 1024) / (int)(SMEM + 1024)
+                                    : 1;
+  static constexpr int RFIT   = 65536 / (MINB * THREADS) / 8 * 8;
+  static constexpr int MAXREG = RFIT > 255 ? 255 : RFIT;
   // pass C's rows (n^3 elements at i_1 n^5 + i_2 n^4 + r n^3) are whole
   // 16-byte units: bulk reduce-adds from the staging buffer
   static constexpr bool ROWS16 = (N3 * sizeof(T)) % 16 == 0;
@@ -281,19 +293,19 @@ __device__ __forceinline__ void pass_b(T *slab, const T *As, int f)
 }
 
 template <typename T, int N>
-__global__ void __launch_bounds__(SlabShape<T, N>::THREADS, SlabShape<T, N>::MINB)
+__global__ void __maxnreg__((SlabShape<T, N>::MAXREG))
     kron_slab_kernel(const __grid_constant__ Params p, int *status, long long spin,
                      long long drain, int flags)
 {
   using S            = SlabShape<T, N>;
   constexpr int CS   = S::CS;
+  constexpr int NS   = S::NS;
   constexpr int N2   = S::N2, N3 = S::N3, N4 = S::N4, N5 = S::N5, ASZ = S::ASZ;
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
-  int *dead_mark = reinterpret_cast<int *>(smem + 16);
-  int *sflags    = reinterpret_cast<int *>(smem + 20);
-  int *peer_dead = reinterpret_cast<int *>(smem + 28);
-  T *obuf        = reinterpret_cast<T *>(smem + S::OFF_OUT);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + S::OFF_BARS);
+  int *dead_mark = reinterpret_cast<int *>(smem + S::OFF_DEAD);
+  int *peer_dead = reinterpret_cast<int *>(smem + S::OFF_PEER_DEAD);
+  int *sflags    = reinterpret_cast<int *>(smem + S::OFF_FLAGS);
   auto stage_x   = [&](int s) {
     return reinterpret_cast<T *>(smem + S::OFF_STAGE0 + s * S::STAGE_BYTES);
   };
@@ -303,8 +315,8 @@ __global__ void __launch_bounds__(SlabShape<T, N>::THREADS, SlabShape<T, N>::MIN
   const int tid     = threadIdx.x;
   const int rank    = (int)cluster_ctarank();
   const bool rotate = !(flags & KRON_SLAB_NO_ROTATE);
-  const int cid  = blockIdx.x / CS;
-  const int ncl  = gridDim.x / CS;
+  const int cid     = blockIdx.x / CS;
+  const int ncl     = gridDim.x / CS;
   const long long tot = p.eend - p.ebase;
   const int eb = p.ebase + (int)(tot * cid / ncl);
   const int ee = p.ebase + (int)(tot * (cid + 1) / ncl);
@@ -313,8 +325,8 @@ __global__ void __launch_bounds__(SlabShape<T, N>::THREADS, SlabShape<T, N>::MIN
 
   if (tid == 0)
   {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    for (int s = 0; s < NS; s++)
+      mbar_init(&bars[s], 1);
     *dead_mark = 0;
     *peer_dead = 0;
     fence_mbar_init();
@@ -338,7 +350,6 @@ __global__ void __launch_bounds__(SlabShape<T, N>::THREADS, SlabShape<T, N>::MIN
     sflags[s] = (x_tma ? FLAG_X_TMA : 0) | (a_tma ? FLAG_A_TMA : 0);
     const unsigned bytes =
         (x_tma ? (unsigned)S::XB : 0u) + (a_tma ? (unsigned)(ASZ * sizeof(T)) : 0u);
-    fence_proxy_async();
     mbar_expect_tx(&bars[s], bytes);
     if (x_tma)
       tma_load_1d(stage_x(s), xs, (unsigned)S::XB, &bars[s]);
@@ -415,14 +426,27 @@ __global__ void __launch_bounds__(SlabShape<T, N>::THREADS, SlabShape<T, N>::MIN
   const unsigned dead_addr = smem_addr(dead_mark);
   for (int e = eb; e < ee; ++e)
   {
-    const int s     = (e - eb) & 1;
+    const int i     = e - eb;
+    const int s     = i % NS;
+    const int s1    = (i + 1) % NS;
     const bool more = e + 1 < ee;
     // pass A of the next position while barrier 1 settles
     if (more)
     {
-      acquire(e + 1, s ^ 1);
+      acquire(e + 1, s1);
       if (tid < N3)
-        pass_a<T, N>(stage_x(s ^ 1), stage_a(s ^ 1), tid, rotate);
+        pass_a<T, N>(stage_x(s1), stage_a(s1), tid, rotate);
+    }
+    // refill the stage of position e - 1 (the same as e + 2's) with
+    // position e + 2: every block finished reading it at barrier 2 (e - 1),
+    // and its staged results have left once the last bulk group has read
+    // them (issued a pass ago) -- so the copy has about an iteration to land.
+    // Barrier 1 (e) does not wait for thread 0 here: every thread arrived on
+    // it in the previous iteration.
+    if (tid == 0 && !dead && e + 2 < ee)
+    {
+      bulk_wait_read();
+      issue(e + 2, (i + 2) % NS);
     }
     cluster_wait(); // barrier 1 (e): every block finished pass B(e)
     if (tid == 0)
@@ -448,42 +472,29 @@ __global__ void __launch_bounds__(SlabShape<T, N>::THREADS, SlabShape<T, N>::MIN
           v[a * N + c] = ld_cluster<T>(base + (unsigned)((c * N4 + t) * sizeof(T)));
       }
     }
-    // this thread's generic accesses to stage s come before the refill's
-    // bulk copy into it
-    fence_proxy_async();
     cluster_arrive(); // barrier 2 (e): this block's reads of the slabs are done
     if (tid < N3)
     {
       apply_fast<T, N>(v, stage_a(s) + 1 * N2);
       apply_slow<T, N>(v, stage_a(s) + 0 * N2);
     }
+    __syncthreads(); // pass A(e+1) done block-wide; the dead marks are in
+    dead = dead || (*peer_dead != 0);
+    if (more && tid < N3)
+      pass_b<T, N>(stage_x(s1), stage_a(s1), tid);
     T *y            = entry_y<T>(p, entry_index(p, e)) + (long long)rank * N3;
     const bool bulk = S::ROWS16 && aligned16(y);
-    if (tid == 0)
-      bulk_wait_read(); // the previous position's rows have left the staging buffer
-    __syncthreads();
-    dead = dead || (*peer_dead != 0);
+    cluster_wait(); // barrier 2 (e): no block reads this block's stage s any more
     if (!dead)
     {
       if (bulk)
       {
+        // results as rows (i_1, i_2) of n^3 elements over the slab just read
+        T *rows = stage_x(s);
         if (tid < N3)
 #pragma unroll
           for (int q = 0; q < N2; q++)
-            obuf[q * N3 + tid] = v[q];
-        fence_proxy_async();
-        __syncthreads();
-        if (tid == 0)
-        {
-#pragma unroll 1
-          for (int q = 0; q < N2; q++)
-          {
-            const int a = q / N, c = q - a * N;
-            bulk_reduce_add<T>(y + (long long)a * N5 + (long long)c * N4, obuf + q * N3,
-                               (unsigned)(N3 * sizeof(T)));
-          }
-          bulk_commit();
-        }
+            rows[q * N3 + tid] = v[q];
       }
       else if (tid < N3)
       {
@@ -495,11 +506,22 @@ __global__ void __launch_bounds__(SlabShape<T, N>::THREADS, SlabShape<T, N>::MIN
         }
       }
     }
-    if (more && tid < N3)
-      pass_b<T, N>(stage_x(s ^ 1), stage_a(s ^ 1), tid);
-    cluster_wait(); // barrier 2 (e): no block reads this block's stage s any more
-    if (tid == 0 && !dead && e + 2 < ee)
-      issue(e + 2, s);
+    // this thread's generic accesses to stage s come before the bulk
+    // reduce-adds that read it and the copy that later refills it
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0 && !dead && bulk)
+    {
+      const T *rows = stage_x(s);
+#pragma unroll 1
+      for (int q = 0; q < N2; q++)
+      {
+        const int a = q / N, c = q - a * N;
+        bulk_reduce_add<T>(y + (long long)a * N5 + (long long)c * N4, rows + q * N3,
+                           (unsigned)(N3 * sizeof(T)));
+      }
+      bulk_commit();
+    }
     if (more)
       cluster_arrive(); // barrier 1 (e+1)
   }
@@ -507,7 +529,7 @@ __global__ void __launch_bounds__(SlabShape<T, N>::THREADS, SlabShape<T, N>::MIN
   if (tid == 0)
   {
     if (dead)
-      for (int s = 0; s < 2; s++)
+      for (int s = 0; s < NS; s++)
         if ((inflight >> s) & 1)
           mbar_wait_bounded(&bars[s], (phase >> s) & 1, drain);
     bulk_wait_all();
