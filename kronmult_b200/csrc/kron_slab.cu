@@ -12,25 +12,25 @@
 //   pass C  modes 1, 2: block r takes the n^3 tuples t = (i_3..i_6) in
 //           [r n^3, (r+1) n^3) and reads the n^2 elements slab_{i_1}[i_2 n^4 +
 //           t] from the cluster's shared memory (ld.shared::cluster).
-// Once every block has read the slabs, pass C's results go over the block's
-// own slab as n^2 rows (i_1, i_2) of n^3 contiguous elements, and into y by
-// one TMA bulk reduce-add per row.  So y is read and written once, in L2, and
-// outputs that alias add up.
+// Pass C's results are added into y straight from registers by
+// fire-and-forget reductions in L2 (red.global.add): y is read and written
+// once, in L2, outputs that alias add up, and the adds drain while the block
+// goes on with the next entry.
 //
 // Each block keeps a ring of three stages (x slab + factors): the entry being
-// computed, the next one (already landed), and the one after it, whose copy
-// is issued at the start of an iteration into the stage the previous entry
-// just left, so every copy has a whole iteration to land.  The cluster
+// computed, the next one (already landed) and the one after it.  A stage is
+// refilled as soon as every block has read it, with the entry three places
+// ahead, so every copy has more than an iteration to land.  The cluster
 // barriers are split so that independent work fills their latency:
 //
-//   [pass A(e+1), refill stage(e-1) with e+2]  wait1(e)  pass C reads(e)
-//   arrive2(e)  [pass C math(e), pass B(e+1)]  wait2(e)
-//   results(e) over stage(e), bulk reduce-adds;  arrive1(e+1) ...
+//   [pass A(e+1)]  wait1(e)  pass C reads(e)  arrive2(e)
+//   [pass C math(e), pass B(e+1)]  wait2(e)  arrive1(e+1)
+//   refill stage(e) with e+3;  y += results(e) ...
 //
 // Barrier 1 of entry e: every block has finished pass B(e), so pass C may
 // read.  Barrier 2 of entry e: every block has finished reading the others'
-// slabs of e, so the slab can take the results, the stage can be refilled
-// later, and no block leaves while another still reads it.
+// slabs of e, so the stage can be refilled and no block leaves while another
+// still reads it.
 //
 // Every mbarrier wait is bounded (wait_limit() polls).  A block whose copies
 // do not arrive in time does four things:
@@ -89,9 +89,6 @@ struct SlabShape
                                     : 1;
   static constexpr int RFIT   = 65536 / (MINB * THREADS) / 8 * 8;
   static constexpr int MAXREG = RFIT > 255 ? 255 : RFIT;
-  // pass C's rows (n^3 elements at i_1 n^5 + i_2 n^4 + r n^3) are whole
-  // 16-byte units: bulk reduce-adds from the staging buffer
-  static constexpr bool ROWS16 = (N3 * sizeof(T)) % 16 == 0;
   static constexpr bool XTMA   = XB % 16 == 0;
   static_assert(N3 <= 1024, "one fibre per thread");
 };
@@ -348,6 +345,7 @@ __global__ void __maxnreg__((SlabShape<T, N>::MAXREG))
     const bool a_tma = (p.layout == LAYOUT_BATCHED || p.layout == LAYOUT_PBATCHED) &&
                        (ASZ * sizeof(T)) % 16 == 0 && aligned16(en.A[0]);
     sflags[s] = (x_tma ? FLAG_X_TMA : 0) | (a_tma ? FLAG_A_TMA : 0);
+    fence_proxy_async();
     const unsigned bytes =
         (x_tma ? (unsigned)S::XB : 0u) + (a_tma ? (unsigned)(ASZ * sizeof(T)) : 0u);
     mbar_expect_tx(&bars[s], bytes);
@@ -408,11 +406,8 @@ __global__ void __maxnreg__((SlabShape<T, N>::MAXREG))
   };
 
   if (tid == 0)
-  {
-    issue(eb, 0);
-    if (eb + 1 < ee)
-      issue(eb + 1, 1);
-  }
+    for (int k = 0; k < NS && eb + k < ee; k++)
+      issue(eb + k, k);
 
   // passes A and B of the first position
   acquire(eb, 0);
@@ -436,17 +431,6 @@ __global__ void __maxnreg__((SlabShape<T, N>::MAXREG))
       acquire(e + 1, s1);
       if (tid < N3)
         pass_a<T, N>(stage_x(s1), stage_a(s1), tid, rotate);
-    }
-    // refill the stage of position e - 1 (the same as e + 2's) with
-    // position e + 2: every block finished reading it at barrier 2 (e - 1),
-    // and its staged results have left once the last bulk group has read
-    // them (issued a pass ago) -- so the copy has about an iteration to land.
-    // Barrier 1 (e) does not wait for thread 0 here: every thread arrived on
-    // it in the previous iteration.
-    if (tid == 0 && !dead && e + 2 < ee)
-    {
-      bulk_wait_read();
-      issue(e + 2, (i + 2) % NS);
     }
     cluster_wait(); // barrier 1 (e): every block finished pass B(e)
     if (tid == 0)
@@ -478,62 +462,37 @@ __global__ void __maxnreg__((SlabShape<T, N>::MAXREG))
       apply_fast<T, N>(v, stage_a(s) + 1 * N2);
       apply_slow<T, N>(v, stage_a(s) + 0 * N2);
     }
+    // this thread is done with stage s (pass B wrote it, pass C read it and
+    // its factors): its generic accesses come before the copy that refills it
+    fence_proxy_async();
     __syncthreads(); // pass A(e+1) done block-wide; the dead marks are in
     dead = dead || (*peer_dead != 0);
     if (more && tid < N3)
       pass_b<T, N>(stage_x(s1), stage_a(s1), tid);
-    T *y            = entry_y<T>(p, entry_index(p, e)) + (long long)rank * N3;
-    const bool bulk = S::ROWS16 && aligned16(y);
+    T *y = entry_y<T>(p, entry_index(p, e)) + (long long)rank * N3;
     cluster_wait(); // barrier 2 (e): no block reads this block's stage s any more
-    if (!dead)
+    if (more)
+      cluster_arrive(); // barrier 1 (e+1): pass B(e+1) is done
+    // stage s is free: it takes position e + 3, more than an iteration ahead
+    if (tid == 0 && !dead && e + NS < ee)
+      issue(e + NS, s);
+    // y += results: fire-and-forget adds in L2 (each element of y gets one
+    // add from this launch unless outputs alias, which the adds also cover)
+    if (!dead && tid < N3)
     {
-      if (bulk)
-      {
-        // results as rows (i_1, i_2) of n^3 elements over the slab just read
-        T *rows = stage_x(s);
-        if (tid < N3)
 #pragma unroll
-          for (int q = 0; q < N2; q++)
-            rows[q * N3 + tid] = v[q];
-      }
-      else if (tid < N3)
-      {
-#pragma unroll
-        for (int q = 0; q < N2; q++)
-        {
-          const int a = q / N, c = q - a * N;
-          atomicAdd(y + (long long)a * N5 + (long long)c * N4 + tid, v[q]);
-        }
-      }
-    }
-    // this thread's generic accesses to stage s come before the bulk
-    // reduce-adds that read it and the copy that later refills it
-    fence_proxy_async();
-    __syncthreads();
-    if (tid == 0 && !dead && bulk)
-    {
-      const T *rows = stage_x(s);
-#pragma unroll 1
       for (int q = 0; q < N2; q++)
       {
         const int a = q / N, c = q - a * N;
-        bulk_reduce_add<T>(y + (long long)a * N5 + (long long)c * N4, rows + q * N3,
-                           (unsigned)(N3 * sizeof(T)));
+        red_add(y + (long long)a * N5 + (long long)c * N4 + tid, v[q]);
       }
-      bulk_commit();
     }
-    if (more)
-      cluster_arrive(); // barrier 1 (e+1)
   }
 
-  if (tid == 0)
-  {
-    if (dead)
-      for (int s = 0; s < NS; s++)
-        if ((inflight >> s) & 1)
-          mbar_wait_bounded(&bars[s], (phase >> s) & 1, drain);
-    bulk_wait_all();
-  }
+  if (tid == 0 && dead)
+    for (int s = 0; s < NS; s++)
+      if ((inflight >> s) & 1)
+        mbar_wait_bounded(&bars[s], (phase >> s) & 1, drain);
 }
 
 template <typename T, int N>
