@@ -351,11 +351,13 @@ int kron_l2_persist_reset(kron_stream_t stream);
  *                       the bit, when the caller passes no W)
  *   KRON_VARIANT_LARGE  two-phase launches through the workspace W
  *   KRON_VARIANT_SLAB   slab-cluster kernel for d = 6, n = 6 (FP64 and
- *                       FP32): one cluster of n blocks per entry, each block
- *                       holding one n^5 slab, no workspace; param
- *                       KRON_SLAB_NO_ROTATE turns off the lane rotation that
- *                       keeps its first FP64 pass free of bank conflicts (a
- *                       comparison form)
+ *                       FP32): one cluster of 12 blocks per entry, each
+ *                       block holding half of one n^5 slab, no workspace;
+ *                       param bits (comparison forms): KRON_SLAB_WHOLE --
+ *                       clusters of 6 blocks holding whole slabs;
+ *                       KRON_SLAB_NO_ROTATE -- no lane rotation in its first
+ *                       FP64 pass (which keeps that pass free of bank
+ *                       conflicts)
  * kron_autotune times every variant that runs (d, n, precision) on a
  * synthetic batched problem of up to batchCount entries (capped at 1 GiB),
  * records the fastest for that key and returns it (outputs may be NULL).
@@ -382,6 +384,7 @@ int kron_l2_persist_reset(kron_stream_t stream);
 #define KRON_BIG_CUDA_CORES 256
 #define KRON_BIG_SMEM_W 512
 #define KRON_SLAB_NO_ROTATE 1
+#define KRON_SLAB_WHOLE 2
 
 int kron_autotune(int d, int n, int precision, int batchCount, int *variant, int *param,
                   double *best_us, kron_stream_t stream);

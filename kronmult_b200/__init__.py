@@ -246,6 +246,8 @@ BIG_CUDA_CORES = 256
 BIG_SMEM_W = 512
 # "slab" param bit: no lane rotation in the first FP64 pass (comparison form)
 SLAB_NO_ROTATE = 1
+# "slab" param bit: clusters of 6 blocks holding whole slabs (comparison form)
+SLAB_WHOLE = 2
 
 
 def autotune(d, n, precision="f64", batch=1024, stream=None):

@@ -58,18 +58,24 @@ namespace {
 
 using namespace ptx;
 
-template <typename T, int N>
+// H: blocks per slab.  Block r of the cluster holds part r % H of slab
+// r / H: i_1 = r / H and the n / H values of i_2 from (r % H) n / H on,
+// n^5 / H contiguous elements of x.
+template <typename T, int N, int H>
 struct SlabShape
 {
-  static constexpr int CS      = N; // blocks per cluster, one slab each
+  static_assert(N % H == 0, "slabs split evenly");
+  static constexpr int CS      = N * H; // blocks per cluster
   static constexpr int N2      = N * N;
   static constexpr int N3      = N2 * N;
   static constexpr int N4      = N3 * N;
   static constexpr int N5      = N4 * N;
-  static constexpr int FIB     = N3; // fibres of every pass (pass C: tuples)
+  static constexpr int NL      = N / H;  // values of i_2 in a block
+  static constexpr int PART    = N5 / H; // elements of x in a block
+  static constexpr int FIB     = N3 / H; // fibres of every pass (pass C: tuples)
   static constexpr int THREADS = (FIB + 31) / 32 * 32;
   static constexpr int ASZ     = 6 * N2;
-  static constexpr size_t XB   = (size_t)N5 * sizeof(T);
+  static constexpr size_t XB   = (size_t)PART * sizeof(T);
   static constexpr size_t AB   = ((size_t)ASZ * sizeof(T) + 15) / 16 * 16;
   static constexpr size_t STAGE_BYTES = (XB + AB + 127) / 128 * 128;
   static constexpr int NS      = 3; // stages: computing, landing, being refilled
@@ -90,7 +96,7 @@ struct SlabShape
   static constexpr int RFIT   = 65536 / (MINB * THREADS) / 8 * 8;
   static constexpr int MAXREG = RFIT > 255 ? 255 : RFIT;
   static constexpr bool XTMA   = XB % 16 == 0;
-  static_assert(N3 <= 1024, "one fibre per thread");
+  static_assert(FIB <= 1024, "one fibre per thread");
 };
 
 constexpr int FLAG_X_TMA = 1; // slab arrived by bulk copy
@@ -289,13 +295,14 @@ __device__ __forceinline__ void pass_b(T *slab, const T *As, int f)
       b[a * N3 + c * N2] = v[a * N + c];
 }
 
-template <typename T, int N>
-__global__ void __maxnreg__((SlabShape<T, N>::MAXREG))
+template <typename T, int N, int H>
+__global__ void __maxnreg__((SlabShape<T, N, H>::MAXREG))
     kron_slab_kernel(const __grid_constant__ Params p, int *status, long long spin,
                      long long drain, int flags)
 {
-  using S            = SlabShape<T, N>;
+  using S            = SlabShape<T, N, H>;
   constexpr int CS   = S::CS;
+  constexpr int NL   = S::NL, PART = S::PART, FIB = S::FIB;
   constexpr int NS   = S::NS;
   constexpr int N2   = S::N2, N3 = S::N3, N4 = S::N4, N5 = S::N5, ASZ = S::ASZ;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -340,7 +347,7 @@ __global__ void __maxnreg__((SlabShape<T, N>::MAXREG))
   auto issue = [&](int e, int s) {
     EntryRef<T> en;
     entry_fetch<T>(p, entry_index(p, e), 6, en);
-    const T *xs      = en.x + (long long)rank * N5;
+    const T *xs      = en.x + (long long)rank * PART;
     const bool x_tma = S::XTMA && aligned16(xs);
     const bool a_tma = (p.layout == LAYOUT_BATCHED || p.layout == LAYOUT_PBATCHED) &&
                        (ASZ * sizeof(T)) % 16 == 0 && aligned16(en.A[0]);
@@ -375,9 +382,9 @@ __global__ void __maxnreg__((SlabShape<T, N>::MAXREG))
           entry_fetch<T>(p, entry_index(p, e), 6, en);
           if (!(fl & FLAG_X_TMA))
           {
-            const T *xs = en.x + (long long)rank * N5;
+            const T *xs = en.x + (long long)rank * PART;
             T *sx       = stage_x(s);
-            for (int i = tid; i < N5; i += blockDim.x)
+            for (int i = tid; i < PART; i += blockDim.x)
               sx[i] = xs[i];
           }
           if (!(fl & FLAG_A_TMA))
@@ -411,10 +418,10 @@ __global__ void __maxnreg__((SlabShape<T, N>::MAXREG))
 
   // passes A and B of the first position
   acquire(eb, 0);
-  if (tid < N3)
+  if (tid < FIB)
     pass_a<T, N>(stage_x(0), stage_a(0), tid, rotate);
   __syncthreads();
-  if (tid < N3)
+  if (tid < FIB)
     pass_b<T, N>(stage_x(0), stage_a(0), tid);
   cluster_arrive(); // barrier 1 (eb)
 
@@ -429,7 +436,7 @@ __global__ void __maxnreg__((SlabShape<T, N>::MAXREG))
     if (more)
     {
       acquire(e + 1, s1);
-      if (tid < N3)
+      if (tid < FIB)
         pass_a<T, N>(stage_x(s1), stage_a(s1), tid, rotate);
     }
     cluster_wait(); // barrier 1 (e): every block finished pass B(e)
@@ -444,20 +451,25 @@ __global__ void __maxnreg__((SlabShape<T, N>::MAXREG))
     // pass C: tuple t of every slab of the cluster
     T v[N2];
     const unsigned sbase = smem_addr(stage_x(s));
-    const int t          = rank * N3 + tid;
-    if (tid < N3)
+    const int t          = rank * FIB + tid;
+    if (tid < FIB)
     {
+      // element (i_1 = a, i_2 = c, t) is in block a H + c / NL, at
+      // (c mod NL) n^4 + t of its part
 #pragma unroll
-      for (int a = 0; a < CS; a++)
-      {
-        const unsigned base = mapa(sbase, (unsigned)a);
+      for (int a = 0; a < N; a++)
 #pragma unroll
-        for (int c = 0; c < N; c++)
-          v[a * N + c] = ld_cluster<T>(base + (unsigned)((c * N4 + t) * sizeof(T)));
-      }
+        for (int h = 0; h < H; h++)
+        {
+          const unsigned base = mapa(sbase, (unsigned)(a * H + h));
+#pragma unroll
+          for (int cl = 0; cl < NL; cl++)
+            v[a * N + h * NL + cl] =
+                ld_cluster<T>(base + (unsigned)((cl * N4 + t) * sizeof(T)));
+        }
     }
     cluster_arrive(); // barrier 2 (e): this block's reads of the slabs are done
-    if (tid < N3)
+    if (tid < FIB)
     {
       apply_fast<T, N>(v, stage_a(s) + 1 * N2);
       apply_slow<T, N>(v, stage_a(s) + 0 * N2);
@@ -467,9 +479,9 @@ __global__ void __maxnreg__((SlabShape<T, N>::MAXREG))
     fence_proxy_async();
     __syncthreads(); // pass A(e+1) done block-wide; the dead marks are in
     dead = dead || (*peer_dead != 0);
-    if (more && tid < N3)
+    if (more && tid < FIB)
       pass_b<T, N>(stage_x(s1), stage_a(s1), tid);
-    T *y = entry_y<T>(p, entry_index(p, e)) + (long long)rank * N3;
+    T *y = entry_y<T>(p, entry_index(p, e)) + (long long)rank * FIB;
     cluster_wait(); // barrier 2 (e): no block reads this block's stage s any more
     if (more)
       cluster_arrive(); // barrier 1 (e+1): pass B(e+1) is done
@@ -478,7 +490,7 @@ __global__ void __maxnreg__((SlabShape<T, N>::MAXREG))
       issue(e + NS, s);
     // y += results: fire-and-forget adds in L2 (each element of y gets one
     // add from this launch unless outputs alias, which the adds also cover)
-    if (!dead && tid < N3)
+    if (!dead && tid < FIB)
     {
 #pragma unroll
       for (int q = 0; q < N2; q++)
@@ -495,16 +507,35 @@ __global__ void __maxnreg__((SlabShape<T, N>::MAXREG))
         mbar_wait_bounded(&bars[s], (phase >> s) & 1, drain);
 }
 
-template <typename T, int N>
+template <typename T, int N, int H>
 int launch_slab_t(Params p, int flags, cudaStream_t stream)
 {
-  using S        = SlabShape<T, N>;
-  const void *fn = reinterpret_cast<const void *>(&kron_slab_kernel<T, N>);
+  using S        = SlabShape<T, N, H>;
+  const void *fn = reinterpret_cast<const void *>(&kron_slab_kernel<T, N, H>);
   if (S::SMEM > (size_t)device_info().max_smem_optin)
     return KRON_ERROR_NOT_SUPPORTED;
   int per_sm = 1;
   if (cached_occupancy(fn, S::THREADS, S::SMEM, &per_sm) != KRON_SUCCESS)
     return KRON_ERROR_LAUNCH;
+  if (S::CS > 8)
+  {
+    // clusters above the portable 8 blocks (B200 runs up to 16); set once
+    // per device
+    static bool nonportable_set[64] = {};
+    const int dev = device_info().device;
+    if (dev < 0 || dev >= 64)
+      return KRON_ERROR_NOT_SUPPORTED;
+    if (!nonportable_set[dev])
+    {
+      if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+          cudaSuccess)
+      {
+        cudaGetLastError();
+        return KRON_ERROR_NOT_SUPPORTED;
+      }
+      nonportable_set[dev] = true;
+    }
+  }
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
   attr[0].id               = cudaLaunchAttributeClusterDimension;
@@ -551,8 +582,15 @@ int launch_slab(Params p, int prec, int flags, cudaStream_t stream)
   if (p.eend <= p.ebase)
     return KRON_SUCCESS;
   if (p.n[0] == 6)
-    return prec == PREC_F32 ? launch_slab_t<float, 6>(p, flags, stream)
-                            : launch_slab_t<double, 6>(p, flags, stream);
+  {
+    // half slabs (clusters of 12, two or four blocks per SM) by default;
+    // whole slabs (clusters of 6) on request
+    if (flags & KRON_SLAB_WHOLE)
+      return prec == PREC_F32 ? launch_slab_t<float, 6, 1>(p, flags, stream)
+                              : launch_slab_t<double, 6, 1>(p, flags, stream);
+    return prec == PREC_F32 ? launch_slab_t<float, 6, 2>(p, flags, stream)
+                            : launch_slab_t<double, 6, 2>(p, flags, stream);
+  }
   return KRON_ERROR_NOT_SUPPORTED;
 }
 

@@ -1,13 +1,13 @@
-"""GPU: the slab-cluster kernel (d = 6, n = 6; one cluster of six blocks per
-entry, no workspace) against the oracle, through the C ABI.
+"""GPU: the slab-cluster kernel (d = 6, n = 6; one cluster of twelve blocks
+per entry holding half slabs, or six holding whole slabs; no workspace)
+against the oracle, through the C ABI.
 
 Covers every path of the kernel:
 - both stages of each block's ring, with batches from 1 entry to several
   entries per cluster;
 - the TMA copies and their plain-load fallbacks (x not 16-byte aligned;
   xbatched factors with lda > n);
-- the bulk reduce-adds into y and their atomic fallback (y not 16-byte
-  aligned);
+- results added into y at any alignment (y shifted by one element);
 - outputs that alias (pbatched);
 - FP32 and FP64.
 FP64 bar: normwise relative error <= 1e-13; FP32 <= 1e-5 against the FP64
@@ -44,10 +44,12 @@ def _inputs(batch, seed, ny=None):
 
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 @pytest.mark.parametrize("batch", [1, 7, 40, 150])
-@pytest.mark.parametrize("forced", [None, 0, kb.SLAB_NO_ROTATE])
+@pytest.mark.parametrize("forced", [None, 0, kb.SLAB_NO_ROTATE, kb.SLAB_WHOLE,
+                                    kb.SLAB_WHOLE | kb.SLAB_NO_ROTATE])
 def test_slab_batched(gpu_lib, prec, batch, forced):
     """forced: None = built-in choice, else the slab variant with that param
-    (with and without the lane rotation of its first pass)."""
+    (half or whole slabs per block, with and without the lane rotation of
+    the first pass)."""
     import torch
 
     if forced is not None:
