@@ -12,10 +12,11 @@
 //   pass C  modes 1, 2: block r takes the n^3 tuples t = (i_3..i_6) in
 //           [r n^3, (r+1) n^3) and reads the n^2 elements slab_{i_1}[i_2 n^4 +
 //           t] from the cluster's shared memory (ld.shared::cluster).
-// Pass C's results are added into y straight from registers by
-// fire-and-forget reductions in L2 (red.global.add): y is read and written
-// once, in L2, outputs that alias add up, and the adds drain while the block
-// goes on with the next entry.
+// Pass C's results are added into y straight from registers: y is read and
+// written once.  Distinct outputs (the batched layout) take plain loads of y,
+// prefetched into L2 an entry ahead, and stores; outputs that may alias take
+// fire-and-forget reductions in L2 (red.global.add), which add up.  L2's
+// atomic throughput is well below HBM's, so the distinct form matters.
 //
 // Each block keeps a ring of three stages (x slab + factors): the entry being
 // computed, the next one (already landed) and the one after it.  A stage is
@@ -90,9 +91,9 @@ struct SlabShape
   static_assert(OFF_FLAGS + 4 * NS <= OFF_STAGE0, "header");
   // blocks per SM that the shared memory allows, and the register cap that
   // lets that many blocks of THREADS threads share the 64K registers
-  static constexpr int MINB   = (228 * 1024) / (int)(SMEM + 1024) > 0
-                                    ? (228 * 1024) / (int)(SMEM + 1024)
-                                    : 1;
+  // (at most three: more blocks would leave too few registers per thread)
+  static constexpr int SMEMB  = (228 * 1024) / (int)(SMEM + 1024);
+  static constexpr int MINB   = SMEMB < 1 ? 1 : (SMEMB > 3 ? 3 : SMEMB);
   static constexpr int RFIT   = 65536 / (MINB * THREADS) / 8 * 8;
   static constexpr int MAXREG = RFIT > 255 ? 255 : RFIT;
   static constexpr bool XTMA   = XB % 16 == 0;
@@ -319,6 +320,16 @@ __global__ void __maxnreg__((SlabShape<T, N, H>::MAXREG))
   const int tid     = threadIdx.x;
   const int rank    = (int)cluster_ctarank();
   const bool rotate = !(flags & KRON_SLAB_NO_ROTATE);
+  const bool atomic_y = p.accum != ACC_DISTINCT || (flags & KRON_SLAB_ATOMIC_Y);
+  // this thread's n^2 elements of position e's y into L2
+  auto prefetch_y = [&](const T *yt) {
+#pragma unroll
+    for (int q = 0; q < N2; q++)
+    {
+      const int a = q / N, c = q - a * N;
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(yt + (long long)a * N5 + (long long)c * N4));
+    }
+  };
   const int cid     = blockIdx.x / CS;
   const int ncl     = gridDim.x / CS;
   const long long tot = p.eend - p.ebase;
@@ -416,6 +427,8 @@ __global__ void __maxnreg__((SlabShape<T, N, H>::MAXREG))
     for (int k = 0; k < NS && eb + k < ee; k++)
       issue(eb + k, k);
 
+  if (!atomic_y && tid < FIB)
+    prefetch_y(entry_y<T>(p, entry_index(p, eb)) + (long long)rank * FIB + tid);
   // passes A and B of the first position
   acquire(eb, 0);
   if (tid < FIB)
@@ -488,17 +501,40 @@ __global__ void __maxnreg__((SlabShape<T, N, H>::MAXREG))
     // stage s is free: it takes position e + 3, more than an iteration ahead
     if (tid == 0 && !dead && e + NS < ee)
       issue(e + NS, s);
-    // y += results: fire-and-forget adds in L2 (each element of y gets one
-    // add from this launch unless outputs alias, which the adds also cover)
+    // y += results.  Outputs that may alias: fire-and-forget adds in L2.
+    // Distinct outputs: plain loads (the lines were prefetched into L2 an
+    // iteration ago) and stores -- L2 atomics would cap the whole kernel at
+    // their throughput, well below HBM's
     if (!dead && tid < FIB)
     {
-#pragma unroll
-      for (int q = 0; q < N2; q++)
+      if (atomic_y)
       {
-        const int a = q / N, c = q - a * N;
-        red_add(y + (long long)a * N5 + (long long)c * N4 + tid, v[q]);
+#pragma unroll
+        for (int q = 0; q < N2; q++)
+        {
+          const int a = q / N, c = q - a * N;
+          red_add(y + (long long)a * N5 + (long long)c * N4 + tid, v[q]);
+        }
+      }
+      else
+      {
+        T yv[N2];
+#pragma unroll
+        for (int q = 0; q < N2; q++)
+        {
+          const int a = q / N, c = q - a * N;
+          yv[q]       = y[(long long)a * N5 + (long long)c * N4 + tid];
+        }
+#pragma unroll
+        for (int q = 0; q < N2; q++)
+        {
+          const int a = q / N, c = q - a * N;
+          y[(long long)a * N5 + (long long)c * N4 + tid] = yv[q] + v[q];
+        }
       }
     }
+    if (!atomic_y && !dead && more && tid < FIB)
+      prefetch_y(entry_y<T>(p, entry_index(p, e + 1)) + (long long)rank * FIB + tid);
   }
 
   if (tid == 0 && dead)
