@@ -348,7 +348,9 @@ int kron_l2_persist_reset(kron_stream_t stream);
  *                       KRON_BIG_SMEM_W to keep the intermediate in the
  *                       cluster's shared memory instead of the workspace W
  *                       (FP64 d = 6, n = 6; that form also runs, without
- *                       the bit, when the caller passes no W)
+ *                       the bit, when the caller passes no W), plus
+ *                       KRON_BIG_NO_L2_HINTS to drop the L2 cache policies
+ *                       that keep W resident (a comparison form)
  *   KRON_VARIANT_LARGE  two-phase launches through the workspace W
  *   KRON_VARIANT_SLAB   slab-cluster kernel for d = 6, n = 6 (FP64 and
  *                       FP32): one cluster of 12 blocks per entry, each
@@ -384,6 +386,7 @@ int kron_l2_persist_reset(kron_stream_t stream);
 #define KRON_VARIANT_SLAB 7
 #define KRON_BIG_CUDA_CORES 256
 #define KRON_BIG_SMEM_W 512
+#define KRON_BIG_NO_L2_HINTS 1024
 #define KRON_SLAB_NO_ROTATE 1
 #define KRON_SLAB_WHOLE 2
 #define KRON_SLAB_ATOMIC_Y 4

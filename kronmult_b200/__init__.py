@@ -244,6 +244,8 @@ BIG_CUDA_CORES = 256
 # "big" param bit: keep the intermediate in the cluster's shared memory
 # instead of the workspace W (FP64 d = 6, n = 6)
 BIG_SMEM_W = 512
+# "big" param bit: no L2 cache policies on W, x and y (comparison form)
+BIG_NO_L2_HINTS = 1024
 # "slab" param bit: no lane rotation in the first FP64 pass (comparison form)
 SLAB_NO_ROTATE = 1
 # "slab" param bit: clusters of 6 blocks holding whole slabs (comparison form)

@@ -14,7 +14,9 @@
 // This is the recursive algorithm's two-level split (kronmultv_recur.hpp:
 // 117-145 applies A_1 on X viewed as (n2..nd) x n1, then recurses), with
 // the intermediate W kept L2-resident: only one entry per cluster is in
-// flight, so the live W is (#clusters x n^d) elements.  The next entry's x
+// flight, so the live W is (#clusters x n^d) elements, and W is written with
+// an evict-last L2 policy while x, y and W's read-back take evict-first, so
+// the streaming operands do not push W out to HBM before phase 2 reads it.  The next entry's x
 // and this entry's y are prefetched into L2 while the cluster computes.
 #include <algorithm>
 #include <cstdint>
@@ -71,7 +73,86 @@ struct BigWS
   long long stride;     // elements between slots (base form)
   void *const *ptrs;    // pointer form
   int per_entry;        // 1: a slot per entry; 0: a slot per cluster
+  int l2_hints;         // 1: W written evict-last, x and y streamed evict-first
 };
+
+// L2 cache policies.  The intermediate W of the clusters in flight (tens of
+// MB) fits the 126 MB L2, but x and y stream past it at several TB/s and
+// would push it out before phase 2 reads it back; W's stores carry
+// evict-last, the streaming x loads, W's read-back and y's adds evict-first.
+// Without hints both policies are evict-normal.
+struct L2Pol
+{
+  uint64_t keep, stream;
+};
+
+__device__ __forceinline__ L2Pol make_policies(bool hints)
+{
+  L2Pol p;
+  if (hints)
+  {
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p.keep));
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p.stream));
+  }
+  else
+  {
+    asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p.keep));
+    p.stream = p.keep;
+  }
+  return p;
+}
+
+template <typename T>
+__device__ __forceinline__ void st_pol(T *p, T v, uint64_t pol)
+{
+  if constexpr (sizeof(T) == 8)
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(v), "l"(pol)
+                 : "memory");
+  else
+    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(pol)
+                 : "memory");
+}
+
+// 16 bytes from shared-memory-resident registers to global
+template <typename T>
+__device__ __forceinline__ void st16_pol(T *p, const T *v, uint64_t pol)
+{
+  if constexpr (sizeof(T) == 8)
+    asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p), "d"(v[0]),
+                 "d"(v[1]), "l"(pol)
+                 : "memory");
+  else
+    asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p),
+                 "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "l"(pol)
+                 : "memory");
+}
+
+__device__ __forceinline__ double2 ld16_pol(const double *p, uint64_t pol)
+{
+  double2 r;
+  asm volatile("ld.global.nc.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+               : "=d"(r.x), "=d"(r.y)
+               : "l"(p), "l"(pol));
+  return r;
+}
+
+__device__ __forceinline__ double ld_pol(const double *p, uint64_t pol)
+{
+  double r;
+  asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(r) : "l"(p), "l"(pol));
+  return r;
+}
+
+template <typename T>
+__device__ __forceinline__ void red_pol(T *p, T v, uint64_t pol)
+{
+  if constexpr (sizeof(T) == 8)
+    asm volatile("red.global.add.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(p), "d"(v), "l"(pol)
+                 : "memory");
+  else
+    asm volatile("red.global.add.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(pol)
+                 : "memory");
+}
 
 template <typename T>
 __device__ __forceinline__ T *big_slot(const BigWS &ws, int k, int e, int ebase, int cid)
@@ -126,6 +207,26 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src)
 {
   unsigned s = (unsigned)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(src) : "memory");
+}
+template <typename T>
+__device__ __forceinline__ void cp_async_elem_pol(T *dst, const T *src, uint64_t pol)
+{
+  unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 8, %2;" ::"r"(s),
+                 "l"(src), "l"(pol)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 4, %2;" ::"r"(s),
+                 "l"(src), "l"(pol)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async16_pol(void *dst, const void *src, uint64_t pol)
+{
+  unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(s),
+               "l"(src), "l"(pol)
+               : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ bool al16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
@@ -208,6 +309,7 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
   T *rbuf0 = reinterpret_cast<T *>(smem + S::OFF_R);
   T *tbuf0 = reinterpret_cast<T *>(smem + S::OFF_TILE);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const L2Pol pol = make_policies(ws.l2_hints != 0);
 
   const int cs   = (int)cluster_size();
   const int rank = (int)cluster_rank();
@@ -269,14 +371,14 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
           const double *src = xb + q * 64 + g * 8 + 2 * t;
           if (al16)
           {
-            double2 u = __ldg(reinterpret_cast<const double2 *>(src));
-            v[q][0]   = u.x;
-            v[q][1]   = u.y;
+            const double2 u = ld16_pol(src, pol.stream);
+            v[q][0]         = u.x;
+            v[q][1]         = u.y;
           }
           else
           {
-            v[q][0] = __ldg(src);
-            v[q][1] = __ldg(src + 1);
+            v[q][0] = ld_pol(src, pol.stream);
+            v[q][1] = ld_pol(src + 1, pol.stream);
           }
         }
       };
@@ -301,7 +403,7 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
         for (int q = 0; q < 8; q++)
 #pragma unroll
           for (int pp = 0; pp < 2; pp++)
-            wb[(2 * t + pp) * 64 + q * 8 + g] = acc[q][pp];
+            st_pol(wb + (2 * t + pp) * 64 + q * 8 + g, acc[q][pp], pol.keep);
       }
     }
     else
@@ -314,10 +416,10 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
         const T *src = en.x + (long long)h0 * LT;
         if ((LT * sizeof(T)) % 16 == 0 && al16(src))
           for (int q = tid; q < nr * LT / V; q += BIG_THREADS)
-            cp_async16(buf + q * V, src + q * V);
+            cp_async16_pol(buf + q * V, src + q * V, pol.stream);
         else
           for (int q = tid; q < nr * LT; q += BIG_THREADS)
-            cp_async_elem(buf + q, src + q);
+            cp_async_elem_pol(buf + q, src + q, pol.stream);
         cp_commit();
       };
       int cur = 0;
@@ -339,13 +441,12 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
         T *dst = w + (long long)h0 * LT;
         if ((LT * sizeof(T)) % 16 == 0 && al16(dst))
         {
-          using VT = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
           for (int q = tid; q < nr * LT / V; q += BIG_THREADS)
-            reinterpret_cast<VT *>(dst)[q] = reinterpret_cast<const VT *>(buf)[q];
+            st16_pol(dst + q * V, buf + q * V, pol.keep);
         }
         else
           for (int q = tid; q < nr * LT; q += BIG_THREADS)
-            dst[q] = buf[q];
+            st_pol(dst + q, buf[q], pol.keep);
         __syncthreads();
         cur ^= 1;
       }
@@ -375,7 +476,7 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
         {
           const int h = q / C, c = q - (q / C) * C;
           if (c < cc)
-            cp_async_elem(tile + c * PITCH + h, wd + (long long)h * LT + c0 + c);
+            cp_async_elem_pol(tile + c * PITCH + h, wd + (long long)h * LT + c0 + c, pol.stream);
           else
             tile[c * PITCH + h] = 0.0;
         }
@@ -426,7 +527,7 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
           if (c < cc)
           {
             const int pos = ((i >> 3) & 7) * 64 + (i & 7) * 8 + (i >> 6);
-            red_add(yd + (long long)i * LT + c0 + c, tile[c * PITCH + pos]);
+            red_pol(yd + (long long)i * LT + c0 + c, tile[c * PITCH + pos], pol.stream);
           }
         }
         __syncthreads();
@@ -446,13 +547,14 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
           {
             const int h = (q * V) / C, c = q * V - h * C;
             if (c + V <= cc)
-              cp_async16(buf + q * V, w + (long long)h * LT + c0 + c);
+              cp_async16_pol(buf + q * V, w + (long long)h * LT + c0 + c, pol.stream);
             else
 #pragma unroll
               for (int u = 0; u < V; u++)
               {
                 if (c + u < cc)
-                  cp_async_elem(buf + q * V + u, w + (long long)h * LT + c0 + c + u);
+                  cp_async_elem_pol(buf + q * V + u, w + (long long)h * LT + c0 + c + u,
+                                    pol.stream);
                 else
                   buf[q * V + u] = T(0);
               }
@@ -462,7 +564,7 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
           {
             const int h = q / C, c = q - (q / C) * C;
             if (c < cc)
-              cp_async_elem(buf + q, w + (long long)h * LT + c0 + c);
+              cp_async_elem_pol(buf + q, w + (long long)h * LT + c0 + c, pol.stream);
             else
               buf[q] = T(0);
           }
@@ -489,7 +591,7 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB)
         {
           const int i = q / C, c = q - (q / C) * C;
           if (c < cc)
-            red_add(en.y + (long long)i * LT + c0 + c, tile[q]);
+            red_pol(en.y + (long long)i * LT + c0 + c, tile[q], pol.stream);
         }
         __syncthreads();
         cur ^= 1;
@@ -759,6 +861,7 @@ int launch_big_t(Params p, const Workspace &wsp, int prec, int cluster, cudaStre
   // workspace slots: one per entry when the caller's W has them, else one
   // per cluster
   BigWS ws{};
+  ws.l2_hints              = (cluster & KRON_BIG_NO_L2_HINTS) ? 0 : 1;
   long long nslots_cluster = 1LL << 30;
   if (p.layout == LAYOUT_BATCHED)
   {
@@ -789,7 +892,7 @@ int launch_big_t(Params p, const Workspace &wsp, int prec, int cluster, cudaStre
 
   const long long work = p.eend - p.ebase;
   int cs               = 2;
-  cluster &= ~(KRON_BIG_CUDA_CORES | KRON_BIG_SMEM_W);
+  cluster &= ~(KRON_BIG_CUDA_CORES | KRON_BIG_SMEM_W | KRON_BIG_NO_L2_HINTS);
   if (cluster > 0)
     cs = std::min(8, cluster);
   else if (const char *env = std::getenv("KRON_BIG_CLUSTER"))
