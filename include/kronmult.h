@@ -359,8 +359,8 @@ int kron_l2_persist_reset(kron_stream_t stream);
  *                       clusters of 6 blocks holding whole slabs;
  *                       KRON_SLAB_NO_ROTATE -- no lane rotation in its first
  *                       FP64 pass (which keeps that pass free of bank
- *                       conflicts); KRON_SLAB_ATOMIC_Y -- distinct outputs
- *                       added by L2 atomics instead of loads and stores
+ *                       conflicts); KRON_SLAB_PLAIN_Y -- distinct outputs
+ *                       added by loads and stores instead of L2 atomics
  * kron_autotune times every variant that runs (d, n, precision) on a
  * synthetic batched problem of up to batchCount entries (capped at 1 GiB),
  * records the fastest for that key and returns it (outputs may be NULL).
@@ -389,7 +389,7 @@ int kron_l2_persist_reset(kron_stream_t stream);
 #define KRON_BIG_NO_L2_HINTS 1024
 #define KRON_SLAB_NO_ROTATE 1
 #define KRON_SLAB_WHOLE 2
-#define KRON_SLAB_ATOMIC_Y 4
+#define KRON_SLAB_PLAIN_Y 4
 
 int kron_autotune(int d, int n, int precision, int batchCount, int *variant, int *param,
                   double *best_us, kron_stream_t stream);

@@ -250,8 +250,8 @@ BIG_NO_L2_HINTS = 1024
 SLAB_NO_ROTATE = 1
 # "slab" param bit: clusters of 6 blocks holding whole slabs (comparison form)
 SLAB_WHOLE = 2
-# "slab" param bit: distinct outputs by L2 atomics (comparison form)
-SLAB_ATOMIC_Y = 4
+# "slab" param bit: distinct outputs by loads and stores (comparison form)
+SLAB_PLAIN_Y = 4
 
 
 def autotune(d, n, precision="f64", batch=1024, stream=None):

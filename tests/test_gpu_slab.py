@@ -45,11 +45,11 @@ def _inputs(batch, seed, ny=None):
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 @pytest.mark.parametrize("batch", [1, 7, 40, 150])
 @pytest.mark.parametrize("forced", [None, 0, kb.SLAB_NO_ROTATE, kb.SLAB_WHOLE,
-                                    kb.SLAB_WHOLE | kb.SLAB_NO_ROTATE, kb.SLAB_ATOMIC_Y])
+                                    kb.SLAB_WHOLE | kb.SLAB_NO_ROTATE, kb.SLAB_PLAIN_Y])
 def test_slab_batched(gpu_lib, prec, batch, forced):
     """forced: None = built-in choice, else the slab variant with that param
     (half or whole slabs per block, with and without the lane rotation of
-    the first pass, y by loads and stores or by atomics)."""
+    the first pass, y by atomics or by loads and stores)."""
     import torch
 
     if forced is not None:
