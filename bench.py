@@ -834,6 +834,26 @@ class KgemmBatched(Workload):
         self.kb.kgemm_batched("nn", self.mm, self.nn, self.kk, 1.0, self.pA, self.ldA, self.pB,
                               self.ldB, 1.0, self.pC, self.ldC)
 
+    def comparison(self, torch, timeit):
+        """The same call on the CUDA-core tile kernel (64x64 tiles, FMA) that
+        larger entries use, against the tensor-core kernel of the headline."""
+        self.dY.zero_()
+        self.step()
+        y_tc = self.dY.clone()
+        os.environ["KRON_KGEMM_CUDA_CORES"] = "1"
+        try:
+            ms = timeit(self.step)
+            self.dY.zero_()
+            self.step()
+            torch.cuda.synchronize()
+            err = max_rel_err(torch, self.dY, y_tc)
+        finally:
+            del os.environ["KRON_KGEMM_CUDA_CORES"]
+        return {"cuda_cores": {"ms_per_step": round(ms, 4),
+                               "value": round(self.flops() / ms / 1e6, 2), "unit": "GFLOP/s",
+                               "max_rel_err_vs_tensor_cores": err,
+                               "kernel": "64x64 tiles, K by 16, CUDA-core FMA"}}
+
     def e2e_step(self):
         self.dA.copy_(self.h["A"], non_blocking=True)
         self.dB.copy_(self.h["B"], non_blocking=True)

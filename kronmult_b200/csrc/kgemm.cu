@@ -6,10 +6,15 @@
 // atomics (C of different entries may alias, kgemm_nt.hpp:184-187),
 // beta == 0 stores without reading C, any other beta is a read-modify-write.
 //
-// Design: one 64x64 output tile per block (16x16 threads, 4x4 outputs per
-// thread), K staged through shared memory in steps of 16 with the operand
-// transposes folded into the staging loads, FP64 FMA accumulation.
-#include "kron_internal.cuh"
+// Design: entries up to 64 x 64 x 64 run on the FP64 tensor cores, one entry
+// per block (kgemm_dmma_kernel, below).  Larger entries: one 64x64 output
+// tile per block (16x16 threads, 4x4 outputs per thread), K staged through
+// shared memory in steps of 16 with the operand transposes folded into the
+// staging loads, FP64 FMA accumulation.
+#include <algorithm>
+#include <cstdlib>
+
+#include "kron_launch.h"
 
 namespace kron {
 
@@ -127,6 +132,148 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Entries up to 64 x 64 x 64 on the FP64 tensor cores (mma.sync m8n8k4):
+// one entry per block of four warps at a time, warp w computing the 32 x 32
+// block of C at rows 32 (w / 2), columns 32 (w % 2) as 4 x 4 tiles of 8 x 8
+// held in fragments (D[g][2t], D[g][2t+1] per lane 4g + t), K in steps of 4
+// (A fragment op(A)[g][k], B fragment op(B)[k][g]).  op(A) and op(B) are
+// staged in shared memory, zero padded to whole tiles, in the orientation
+// that keeps both the global reads and the shared writes contiguous (stride
+// 68 doubles, so the fragment reads of either orientation are conflict free:
+// a half-warp's 16 lanes hit words 4g + t or 4t + g mod 16).
+constexpr int DM_THREADS = 128;
+constexpr int DM_S       = 68;
+constexpr int DM_MAX     = 64;
+
+__device__ __forceinline__ void dm_mma(double &d0, double &d1, double a, double b)
+{
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+template <int OP> // 0 = nn, 1 = nt, 2 = tt
+__global__ void __launch_bounds__(DM_THREADS, 3)
+    kgemm_dmma_kernel(int mm, int nn, int kk, double alpha, double *const *Aarr,
+                      const int *ldAarr, double *const *Barr, const int *ldBarr, double beta,
+                      double *const *Carr, const int *ldCarr, int batch)
+{
+  extern __shared__ double dm_smem[];
+  double *As = dm_smem;                // op(A): [k][i] (nn, nt) or [i][k] (tt)
+  double *Bs = dm_smem + DM_MAX * DM_S; // op(B): [j][k] (nn) or [k][j] (nt, tt)
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int mt = (mm + 7) >> 3, nt = (nn + 7) >> 3, kt = (kk + 3) >> 2;
+  const int rows = mt * 8, cols = nt * 8, kp = kt * 4;
+  const int m0 = 4 * (warp >> 1), n0 = 4 * (warp & 1); // first tile of this warp
+  constexpr bool A_KM = OP != 2; // A staged [k][i]
+  constexpr bool B_NK = OP == 0; // B staged [j][k]
+
+  for (int e = blockIdx.x; e < batch; e += gridDim.x)
+  {
+    const double *A     = Aarr[e];
+    const double *B     = Barr[e];
+    double *C           = Carr[e];
+    const long long lda = ldAarr[e], ldb = ldBarr[e], ldc = ldCarr[e];
+    __syncthreads(); // the previous entry's fragments are read
+    for (int q = tid; q < rows * kp; q += DM_THREADS)
+    {
+      if constexpr (A_KM)
+      { // op(A)(i, k) = A[i + k lda]; consecutive threads walk i
+        const int i = q % rows, k = q / rows;
+        As[k * DM_S + i] = (i < mm && k < kk) ? A[i + k * lda] : 0.0;
+      }
+      else
+      { // op(A)(i, k) = A[k + i lda]; consecutive threads walk k
+        const int k = q % kp, i = q / kp;
+        As[i * DM_S + k] = (i < mm && k < kk) ? A[k + i * lda] : 0.0;
+      }
+    }
+    for (int q = tid; q < cols * kp; q += DM_THREADS)
+    {
+      if constexpr (B_NK)
+      { // op(B)(k, j) = B[k + j ldb]; consecutive threads walk k
+        const int k = q % kp, j = q / kp;
+        Bs[j * DM_S + k] = (j < nn && k < kk) ? B[k + j * ldb] : 0.0;
+      }
+      else
+      { // op(B)(k, j) = B[j + k ldb]; consecutive threads walk j
+        const int j = q % cols, k = q / cols;
+        Bs[k * DM_S + j] = (j < nn && k < kk) ? B[j + k * ldb] : 0.0;
+      }
+    }
+    __syncthreads();
+
+    double acc[4][4][2];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++)
+        acc[a][b][0] = acc[a][b][1] = 0.0;
+    for (int ks = 0; ks < kt; ks++)
+    {
+      const int k = ks * 4 + t;
+      double af[4], bf[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+      {
+        const int r = (m0 + u) * 8 + g, c = (n0 + u) * 8 + g;
+        af[u] = (m0 + u < mt) ? (A_KM ? As[k * DM_S + r] : As[r * DM_S + k]) : 0.0;
+        bf[u] = (n0 + u < nt) ? (B_NK ? Bs[c * DM_S + k] : Bs[k * DM_S + c]) : 0.0;
+      }
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+          if (m0 + a < mt && n0 + b < nt) // warp-uniform
+            dm_mma(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++)
+#pragma unroll
+        for (int pp = 0; pp < 2; pp++)
+        {
+          const int i = (m0 + a) * 8 + g, j = (n0 + b) * 8 + 2 * t + pp;
+          if (m0 + a < mt && n0 + b < nt && i < mm && j < nn)
+          {
+            double *c      = C + i + j * ldc;
+            const double v = alpha * acc[a][b][pp];
+            if (beta == 1.0)
+              atomicAdd(c, v);
+            else if (beta == 0.0)
+              *c = v;
+            else
+              *c = beta * (*c) + v;
+          }
+        }
+  }
+}
+
+template <int OP>
+int launch_dmma(int mm, int nn, int kk, double alpha, double *const *A, const int *ldA,
+                double *const *B, const int *ldB, double beta, double *const *C, const int *ldC,
+                int batch, cudaStream_t stream)
+{
+  const void *fn    = reinterpret_cast<const void *>(&kgemm_dmma_kernel<OP>);
+  const size_t smem = 2 * (size_t)DM_MAX * DM_S * sizeof(double);
+  int per_sm        = 1;
+  if (cached_occupancy(fn, DM_THREADS, smem, &per_sm) != KRON_SUCCESS)
+    return KRON_ERROR_LAUNCH;
+  const long long grid =
+      std::max<long long>(1, std::min<long long>(batch, (long long)device_info().sms * per_sm));
+  void *args[] = {&mm, &nn, &kk, &alpha, const_cast<double *const **>(&A),
+                  const_cast<const int **>(&ldA), const_cast<double *const **>(&B),
+                  const_cast<const int **>(&ldB), &beta, const_cast<double *const **>(&C),
+                  const_cast<const int **>(&ldC), &batch};
+  return cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(DM_THREADS), args, smem, stream) ==
+                 cudaSuccess
+             ? KRON_SUCCESS
+             : KRON_ERROR_LAUNCH;
+}
+
 } // namespace
 
 int launch_kgemm(int op, int mm, int nn, int kk, double alpha, double *const *A, const int *ldA,
@@ -135,6 +282,18 @@ int launch_kgemm(int op, int mm, int nn, int kk, double alpha, double *const *A,
 {
   if (batch <= 0 || mm <= 0 || nn <= 0)
     return KRON_SUCCESS;
+  // entries up to 64 x 64 x 64 (the reference tests' sizes) on the FP64
+  // tensor cores, one entry per block
+  if (mm <= DM_MAX && nn <= DM_MAX && kk <= DM_MAX && !std::getenv("KRON_KGEMM_CUDA_CORES"))
+  {
+    switch (op)
+    {
+    case 0: return launch_dmma<0>(mm, nn, kk, alpha, A, ldA, B, ldB, beta, C, ldC, batch, stream);
+    case 1: return launch_dmma<1>(mm, nn, kk, alpha, A, ldA, B, ldB, beta, C, ldC, batch, stream);
+    case 2: return launch_dmma<2>(mm, nn, kk, alpha, A, ldA, B, ldB, beta, C, ldC, batch, stream);
+    default: return KRON_ERROR_INVALID_VALUE;
+    }
+  }
   const int tiles_m = (mm + TM - 1) / TM, tiles_n = (nn + TN - 1) / TN;
   const long long jobs = (long long)tiles_m * tiles_n * batch;
   const int sms        = device_info().sms;

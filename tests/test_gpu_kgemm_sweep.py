@@ -72,3 +72,24 @@ def test_kgemm_beta_one_aliasing_outputs(gpu_lib, op):
     for mm, nn, kk in ((8, 8, 8), (29, 64, 8), (64, 1, 29)):
         err = _case(op, mm, nn, kk, 15, 1.1, 1.0, True, rng)
         assert err <= 1e-13, (op, mm, nn, kk, err)
+
+
+@pytest.mark.parametrize("op", ["nn", "nt", "tt"])
+def test_kgemm_tile_kernel_sizes(gpu_lib, op):
+    """Entries beyond 64 x 64 x 64 take the CUDA-core tile kernel; entries up
+    to it take the tensor-core kernel unless KRON_KGEMM_CUDA_CORES is set,
+    which runs the tile kernel on them too.  Both against the oracle."""
+    import os
+
+    rng = np.random.default_rng({"nn": 31, "nt": 32, "tt": 33}[op])
+    for mm, nn, kk in ((65, 64, 64), (64, 70, 3), (9, 8, 130)):
+        for alpha, beta in ((1.3, 1.2), (1.0, 1.0)):
+            err = _case(op, mm, nn, kk, 5, alpha, beta, False, rng)
+            assert err <= 1e-13, (op, mm, nn, kk, alpha, beta, err)
+    os.environ["KRON_KGEMM_CUDA_CORES"] = "1"
+    try:
+        for mm, nn, kk in ((64, 64, 64), (29, 8, 1)):
+            err = _case(op, mm, nn, kk, 7, 1.3, 1.2, False, rng)
+            assert err <= 1e-13, (op, mm, nn, kk, err)
+    finally:
+        del os.environ["KRON_KGEMM_CUDA_CORES"]
