@@ -153,6 +153,16 @@ __device__ __forceinline__ void dm_mma(double &d0, double &d1, double a, double 
                : "d"(a), "d"(b));
 }
 
+// dst = *src (8 bytes) by an asynchronous copy, or 0 when !valid (zero
+// fill: nothing is read)
+__device__ __forceinline__ void dm_cp8(double *dst, const double *src, bool valid)
+{
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(src),
+               "r"(valid ? 8 : 0)
+               : "memory");
+}
+
 template <int OP> // 0 = nn, 1 = nt, 2 = tt
 __global__ void __launch_bounds__(DM_THREADS, 3)
     kgemm_dmma_kernel(int mm, int nn, int kk, double alpha, double *const *Aarr,
@@ -177,17 +187,20 @@ __global__ void __launch_bounds__(DM_THREADS, 3)
     double *C           = Carr[e];
     const long long lda = ldAarr[e], ldb = ldBarr[e], ldc = ldCarr[e];
     __syncthreads(); // the previous entry's fragments are read
+    // every copy of the entry in flight at once (zero fill outside mm, nn, kk)
     for (int q = tid; q < rows * kp; q += DM_THREADS)
     {
       if constexpr (A_KM)
       { // op(A)(i, k) = A[i + k lda]; consecutive threads walk i
         const int i = q % rows, k = q / rows;
-        As[k * DM_S + i] = (i < mm && k < kk) ? A[i + k * lda] : 0.0;
+        const bool ok = i < mm && k < kk;
+        dm_cp8(As + k * DM_S + i, ok ? A + i + k * lda : A, ok);
       }
       else
       { // op(A)(i, k) = A[k + i lda]; consecutive threads walk k
         const int k = q % kp, i = q / kp;
-        As[i * DM_S + k] = (i < mm && k < kk) ? A[k + i * lda] : 0.0;
+        const bool ok = i < mm && k < kk;
+        dm_cp8(As + i * DM_S + k, ok ? A + k + i * lda : A, ok);
       }
     }
     for (int q = tid; q < cols * kp; q += DM_THREADS)
@@ -195,14 +208,17 @@ __global__ void __launch_bounds__(DM_THREADS, 3)
       if constexpr (B_NK)
       { // op(B)(k, j) = B[k + j ldb]; consecutive threads walk k
         const int k = q % kp, j = q / kp;
-        Bs[j * DM_S + k] = (j < nn && k < kk) ? B[k + j * ldb] : 0.0;
+        const bool ok = j < nn && k < kk;
+        dm_cp8(Bs + j * DM_S + k, ok ? B + k + j * ldb : B, ok);
       }
       else
       { // op(B)(k, j) = B[j + k ldb]; consecutive threads walk j
         const int j = q % cols, k = q / cols;
-        Bs[k * DM_S + j] = (j < nn && k < kk) ? B[j + k * ldb] : 0.0;
+        const bool ok = j < nn && k < kk;
+        dm_cp8(Bs + k * DM_S + j, ok ? B + j + k * ldb : B, ok);
       }
     }
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
     __syncthreads();
 
     double acc[4][4][2];
