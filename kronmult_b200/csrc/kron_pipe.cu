@@ -197,6 +197,7 @@ struct PipeLayout
 constexpr int META_X_TMA  = 1; // x arrived by bulk copy
 constexpr int META_A_TMA  = 2; // A_1..A_d arrived by bulk copy (contiguous)
 constexpr int META_Y_BULK = 4; // y takes the bulk reduce-add
+constexpr int META_Y_PF   = 8; // y's L2 prefetch went out with the copies
 
 // Offset of element base + kk of a fibre.  In a swizzled buffer the XOR
 // swizzle is linear over GF(2) and base, kk occupy disjoint bits (n = 4:
@@ -540,14 +541,18 @@ __global__ void __launch_bounds__(PIPE_THREADS, PipeOcc<T>::value)
   unsigned inflight = 0; // thread 0: stages with copies not yet waited for
   // issue the copies of position e into stage s (thread 0 only) and record
   // which operands the copies carry
-  auto issue = [&](int e, int s) {
+  // pf_y: prefetch y into L2 together with the copies (refills, an entry or
+  // more ahead); the copies issued at launch leave it to the entry's start so
+  // that every block's first x is not queued behind the y lines
+  auto issue = [&](int e, int s, bool pf_y) {
     EntryRef<T> en;
     entry_fetch<T>(p, entry_index(p, e), D, en);
     const bool a_contig =
         (p.layout == LAYOUT_BATCHED || p.layout == LAYOUT_PBATCHED) && tma_ok<T>(en.A[0], ab);
     const bool x_ok = tma_ok<T>(en.x, xb);
     const bool y_ok = tma_ok<T>(en.y, xb);
-    meta[s] = (x_ok ? META_X_TMA : 0) | (a_contig ? META_A_TMA : 0) | (y_ok ? META_Y_BULK : 0);
+    meta[s] = (x_ok ? META_X_TMA : 0) | (a_contig ? META_A_TMA : 0) | (y_ok ? META_Y_BULK : 0) |
+              (y_ok && pf_y ? META_Y_PF : 0);
     unsigned bytes = (x_ok ? (unsigned)xb : 0u) + (a_contig ? (unsigned)ab : 0u);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect_tx(&bars[s], bytes);
@@ -555,7 +560,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PipeOcc<T>::value)
       tma_load(stage_x(s), en.x, (unsigned)xb, &bars[s]);
     if (a_contig)
       tma_load(stage_a(s), en.A[0], (unsigned)ab, &bars[s]);
-    if (y_ok)
+    if (y_ok && pf_y)
       l2_prefetch(en.y, (unsigned)xb);
     inflight |= 1u << s;
   };
@@ -563,7 +568,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PipeOcc<T>::value)
   int ahead = min(nstage, ee - eb);
   if (tid == 0)
     for (int i = 0; i < ahead; i++)
-      issue(eb + i, i);
+      issue(eb + i, i, false);
   unsigned phases = 0; // bit s = parity to wait for on stage s
   int pending_e = -1, pending_s = 0; // stage refill waiting for its reduce to read it
 
@@ -574,9 +579,13 @@ __global__ void __launch_bounds__(PIPE_THREADS, PipeOcc<T>::value)
     // below, after the A preparation (which reads in-bounds shared memory
     // either way)
     const bool done = ptx::mbar_wait_bounded(&bars[s], (phases >> s) & 1, spin);
-    if (tid == 0 && done)
-      inflight &= ~(1u << s);
     const int fl = meta[s];
+    if (tid == 0 && done)
+    {
+      inflight &= ~(1u << s);
+      if ((fl & META_Y_BULK) && !(fl & META_Y_PF))
+        l2_prefetch(entry_y<T>(p, entry_index(p, e)), (unsigned)xb);
+    }
     T *sx        = stage_x(s);
     T *sa        = stage_a(s);
     // operands the bulk copy could not take (block-uniform): plain loads
@@ -633,7 +642,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PipeOcc<T>::value)
     if (tid == 0 && pending_e >= 0)
     {
       bulk_wait_read();
-      issue(pending_e, pending_s);
+      issue(pending_e, pending_s, true);
       pending_e = -1;
     }
 
