@@ -462,10 +462,12 @@ __device__ __forceinline__ bool gen_mode_sized(int nq, int mq, const T *cur, T *
 
 // SIZED: dispatch modes with n_l, m_l <= 8 to compile-time-sized fibre
 // passes (fewer instructions per product, more registers: used by the
-// uneven-batch kernel, whose blocks are limited by shared memory anyway)
+// uneven-batch kernel, whose blocks are limited by shared memory anyway).
+// rows: independent vectors stored one after another in the buffer (an
+// outer index that no mode touches; 1 for a single vector).
 template <typename T, int PREC, bool SIZED = false>
 __device__ void gen_apply_modes(const GenView &v, T *&cur, T *&nxt, const T *As, int C, int t,
-                                int GS, int g)
+                                int GS, int g, int rows = 1)
 {
   // current dims of the applied modes
   int dims[MAXD];
@@ -484,7 +486,7 @@ __device__ void gen_apply_modes(const GenView &v, T *&cur, T *&nxt, const T *As,
   {
     const int q  = v.forward ? step : (v.dd - 1 - step);
     const int mq = v.mm[q], nq = v.nn[q];
-    long long outer = 1, inner = C;
+    long long outer = rows, inner = C;
     for (int u = 0; u < q; u++)
       outer *= dims[u];
     for (int u = q + 1; u < v.dd; u++)

@@ -6,23 +6,27 @@
 // kron_vplan_create (host, once) builds a per-entry descriptor table:
 //   - Alg. 993 order per entry: forward only when strictly cheaper
 //     (kronm.hpp:39-89), and the largest intermediate of that order;
-//   - a class by that size: "warp" (<= 512 elements: one warp per entry,
-//     eight entries per block), "block" (fits the block's shared memory
-//     twice: one block per entry), "huge" (beyond: a two-phase split, head
-//     modes [0, q) and tail modes [q, d), sizes chosen like the uniform
-//     path);
-//   - every huge entry is cut into work items: row items (phase 1: the tail
-//     modes on a range of head rows, written to the entry's own region of
-//     the workspace) and tile items (phase 2: the head modes on a range of
-//     column tiles of that region, added into y), so all SMs share the
-//     largest entries;
-//   - within each list, items sorted by cost, largest first.
-// kron_vplan_execute_async runs one persistent kernel twice: stage 0 takes
-// huge row items, then block-class entries, then warp-class entries from
-// device work counters; stage 1 (after the launch boundary, the only
-// dependency) takes the tile items.  On a non-default stream the counter
-// reset and both launches are captured once into a CUDA graph and replayed
-// while the operand arrays stay the same.
+//   - a class by the shared memory the entry needs (two buffers of that
+//     intermediate plus its factors) against the per-block budget, half of
+//     an SM so that two blocks share each SM: "warp" (<= 512 elements: one
+//     warp per entry), "quad" / "half" / "block" (a quarter, a half or all
+//     of a block per entry), "huge" (beyond: a two-phase split, head modes
+//     [0, q) and tail modes [q, d));
+//   - every huge entry is cut into work items: chunk items (phase 1: the
+//     tail modes on as many head rows as one block's buffers hold, written
+//     to the entry's own region of the workspace) and tile items (phase 2:
+//     the head modes on one column tile of that region, added into y);
+//   - one queue of huge items, largest entries first, where each entry's
+//     tile items follow its chunk items by a lag (a few hundred items, at
+//     most ~40 MB of live regions): a tile item waits (bounded) on its
+//     entry's chunk counter, which by then is normally complete, and the
+//     region it reads is still in L2.
+// kron_vplan_execute_async runs one persistent kernel: the huge queue, then
+// the block, half, quad and warp classes, each from its own device work
+// counter.  All operands reach shared memory by cp.async, so a block keeps
+// every byte of its current item in flight at once.  On a non-default
+// stream the counter reset and the launch are captured once into a CUDA
+// graph and replayed while the operand arrays stay the same.
 #include <algorithm>
 #include <cstring>
 #include <new>
@@ -30,16 +34,19 @@
 #include <vector>
 
 #include "kron_launch.h"
+#include "kron_ptx.cuh"
 
 using namespace kron;
 
 namespace {
 
-constexpr int VP_THREADS  = 256;
-constexpr int VP_WARPS    = VP_THREADS / 32;
-constexpr int WARP_MAX    = 512;   // elements of the largest intermediate, warp class
+constexpr int VP_THREADS = 256;
+constexpr int VP_WARPS   = VP_THREADS / 32;
+constexpr int VP_MINB    = 2;     // blocks per SM the shared-memory budget leaves room for
+constexpr int WARP_MAX   = 512;   // elements of the largest intermediate, warp class
 constexpr int CLS_WARP = 0, CLS_QUAD = 1, CLS_HALF = 2, CLS_BLOCK = 3, CLS_HUGE = 4;
-constexpr int NCLS     = 5;
+constexpr int NCLS   = 5;
+constexpr int NCOUNT = 8;         // work counters ahead of the per-entry chunk counters
 
 struct VDesc
 {
@@ -47,80 +54,122 @@ struct VDesc
   int k;                // entry index (operands at pA[6k + l], pX[k], pY[k])
   unsigned char d, fwd, q, C;  // order; huge: head modes q, tile columns C
   unsigned char m[6], n[6];
-  int mi;               // largest intermediate (elements) of the chosen order
+  int mi;               // buffer elements: the largest intermediate of the chosen
+                        // order (huge: of one chunk of R head rows)
   int mi2;              // huge: phase-2 buffer elements (tile rows x C)
-  unsigned char fwd1, fwd2;         // huge: order of phase 1 / phase 2
-  unsigned char pad[2];             // huge: [0] warp-parallel phase 1, [1] tail factor
-                                    // elements / 16 (rounded up)
+  unsigned char fwd1, fwd2;   // huge: order of the tail / head modes
+  unsigned short R;           // huge: head rows per chunk item
+  int nchunk;                 // huge: chunk items (its tile items wait for all)
 };
 
-// a range [lo, hi) of head rows (phase 1) or column tiles (phase 2) of the
-// huge entry desc[d]
+// kind 0: chunk item, head rows [lo, hi); kind 1: tile item, column tile lo
+// of the huge entry desc[e]
 struct VItem
 {
-  int d, lo, hi, pad;
+  int e, lo, hi, kind;
 };
 
 struct VParams
 {
   const VDesc *desc;          // [huge | block | half | quad | warp]
-  const VItem *items;         // [row items | tile items]
+  const VItem *items;         // the huge queue
   int nhuge, nblock, nhalf, nquad, nwarp;
-  int nrow, ntile;
-  int stage;                  // 0: row items, block and warp classes; 1: tile items
-  int *counters;              // work counters (zeroed before every execution)
+  int nitems;
+  int *counters;              // [0] huge queue, [1] block, [2] warp, [4] half,
+                              // [5] quad; [NCOUNT + i] chunks done of huge entry i
+  int *status;                // the library's device status word
+  long long spin;             // polls before a chunk wait gives up
   const double *const *pA;
   const double *const *pX;
   double *const *pY;
   double *ws;                 // huge class: per-entry regions
-  int block_elems;            // shared elements per block in block mode
+  int budget;                 // shared elements per block
 };
 
-// One entry (or one sub-block view of it) computed by a group of GS threads
-// in the shared buffers b0/b1 (each >= v.max_inter) with factors in As.
-__device__ __forceinline__ void vp_group_entry(const GenView &v, bool strided, const double *x,
-                                               double *out, int accum, double *b0, double *b1,
-                                               double *As, const double *const *A,
-                                               const int *ld, int t, int GS, int g,
-                                               bool load_a = true)
+// 8-byte global -> shared copy through the LSU's asynchronous path
+// (zero-filled when !valid; src must still point into the operand).
+__device__ __forceinline__ void cp8(double *dst, const double *src, bool valid = true)
 {
-  if (load_a)
-  {
-    int o = 0;
-    for (int q = 0; q < v.dd; q++)
-    {
-      const int l = v.mode0 + q, mq = v.mm[q], nq = v.nn[q];
-      for (int u = t; u < mq * nq; u += GS)
-      {
-        const int j = u / mq, i = u - j * mq;
-        As[o + u]   = __ldg(A[l] + i + (long long)j * ld[l]);
-      }
-      o += mq * nq;
-    }
-  }
-  int rows_in = 1, rows_out = 1;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(ptx::smem_addr(dst)),
+               "l"(src), "r"(valid ? 8 : 0)
+               : "memory");
+}
+
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+__device__ __forceinline__ int ld_acquire(const int *p)
+{
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// The view's factors (leading dimension m_l: each contiguous) into As.
+__device__ __forceinline__ void vp_load_factors(const GenView &v, double *As,
+                                                const double *const *A, int t, int GS)
+{
+  int o = 0;
   for (int q = 0; q < v.dd; q++)
   {
-    rows_in *= v.nn[q];
-    rows_out *= v.mm[q];
+    const int sz    = v.mm[q] * v.nn[q];
+    const double *a = A[v.mode0 + q];
+    for (int u = t; u < sz; u += GS)
+      cp8(As + o + u, a + u);
+    o += sz;
   }
-  if (!strided)
-    group_copy_in(b0, x, rows_in, t, GS);
-  else
-    group_copy_tile(b0, x, rows_in, v.C, (int)v.total_cols, v.in_row, t, GS);
+}
+
+// rows consecutive vectors of the view (x contiguous) computed by a group
+// of GS threads in buffers b0 / b1 (each >= rows x the largest
+// intermediate), factors at As; the results go to out (contiguous).
+__device__ __forceinline__ void vp_run(const GenView &v, int rows, const double *x, double *out,
+                                       int accum, double *b0, double *b1, double *As,
+                                       const double *const *A, int t, int GS, int g)
+{
+  vp_load_factors(v, As, A, t, GS);
+  int rin = rows, rout = rows;
+  for (int q = 0; q < v.dd; q++)
+  {
+    rin *= v.nn[q];
+    rout *= v.mm[q];
+  }
+  for (int i = t; i < rin; i += GS)
+    cp8(b0 + i, x + i);
+  cp_wait_all();
   group_sync(g, GS);
   double *cur = b0, *nxt = b1;
-  gen_apply_modes<double, PREC_F64, true>(v, cur, nxt, As, v.C, t, GS, g);
-  if (!strided)
-    group_flush(accum, out, cur, cur, false, rows_out, t, GS);
-  else
-    for (int q = t; q < rows_out * v.C; q += GS)
-    {
-      const int i = q / v.C, c = q - i * v.C;
-      if (c < v.total_cols)
-        y_update(accum, out + i * v.out_row, c, cur[q]);
-    }
+  gen_apply_modes<double, PREC_F64, true>(v, cur, nxt, As, 1, t, GS, g, rows);
+  group_flush(accum, out, cur, cur, false, rout, t, GS);
   group_sync(g, GS);
+}
+
+// One column tile of a huge entry's region: rows of C columns at stride
+// in_row (the first Cc valid, the rest zero-filled), the head modes, and
+// the Cc valid columns added into y (row stride out_row).  Whole block.
+__device__ __forceinline__ void vp_run_tile(const GenView &v, const double *w, long long in_row,
+                                            int C, int Cc, double *y, long long out_row,
+                                            double *b0, double *b1, double *As,
+                                            const double *const *A, int tid)
+{
+  vp_load_factors(v, As, A, tid, VP_THREADS);
+  int rin = 1, rout = 1;
+  for (int q = 0; q < v.dd; q++)
+  {
+    rin *= v.nn[q];
+    rout *= v.mm[q];
+  }
+  const int lane = tid & 31, warp = tid >> 5;
+  for (int h = warp; h < rin; h += VP_WARPS)
+    for (int c = lane; c < C; c += 32)
+      cp8(b0 + h * C + c, w + h * in_row + (c < Cc ? c : 0), c < Cc);
+  cp_wait_all();
+  __syncthreads();
+  double *cur = b0, *nxt = b1;
+  gen_apply_modes<double, PREC_F64, true>(v, cur, nxt, As, C, tid, VP_THREADS, 0);
+  for (int i = warp; i < rout; i += VP_WARPS)
+    for (int c = lane; c < Cc; c += 32)
+      red_add(y + i * out_row + c, cur[i * C + c]);
+  __syncthreads();
 }
 
 __device__ __forceinline__ void vp_view(GenView &v, const VDesc &e, int mode0, int dd)
@@ -139,13 +188,10 @@ __device__ __forceinline__ void vp_view(GenView &v, const VDesc &e, int mode0, i
 }
 
 __device__ __forceinline__ void vp_operands(const VParams &vp, const VDesc &e, const double *A[6],
-                                            int ld[6], const double *&x, double *&y)
+                                            const double *&x, double *&y)
 {
   for (int l = 0; l < 6; l++)
-  {
-    A[l]  = l < e.d ? vp.pA[6LL * e.k + l] : nullptr;
-    ld[l] = l < e.d ? e.m[l] : 1;
-  }
+    A[l] = l < e.d ? vp.pA[6LL * e.k + l] : nullptr;
   x = vp.pX[e.k];
   y = vp.pY[e.k];
 }
@@ -181,17 +227,45 @@ __device__ __forceinline__ int block_take(int *counter, int *s_idx, int tid)
   return idx;
 }
 
+// Thread 0 polls the entry's chunk counter (acquire) until `need` chunk
+// items are done, at most `spin` polls; on giving up it records 1 in the
+// status word.  Returns the outcome to the whole block.
+__device__ __forceinline__ bool vp_wait_chunks(const VParams &vp, int e, int need, int *s_flag,
+                                               int tid)
+{
+  if (tid == 0)
+  {
+    const int *done = vp.counters + NCOUNT + e;
+    int ok          = 1;
+    long long polls = 0;
+    while (ld_acquire(done) < need)
+    {
+      if (++polls > vp.spin)
+      {
+        ok = 0;
+        if (vp.status)
+          atomicExch(vp.status, 1);
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+    *s_flag = ok;
+  }
+  __syncthreads();
+  return *s_flag != 0;
+}
+
 // Entries of one class run by groups of GS threads, VP_THREADS / GS per
-// block, each group with its own slice of shared memory and named barrier.
+// block, each group with its own slice of shared memory and barrier.
 template <int GS>
 __device__ __forceinline__ void group_class(const VParams &vp, const VDesc *list, int n,
                                             int *counter, double *smem, int *s_gidx, int tid)
 {
   constexpr int NG = VP_THREADS / GS;
   const int g = tid / GS, t = tid - (tid / GS) * GS;
-  double *b0  = smem + (long long)g * ((vp.block_elems / NG) & ~1);
+  double *b0  = smem + (long long)g * ((vp.budget / NG) & ~1);
   const double *A[6];
-  int ld[6];
   const double *x;
   double *y;
   while (true)
@@ -206,133 +280,75 @@ __device__ __forceinline__ void group_class(const VParams &vp, const VDesc *list
     const VDesc e = list[idx];
     GenView v;
     vp_view(v, e, 0, e.d);
-    vp_operands(vp, e, A, ld, x, y);
-    const int mi = (e.mi + 1) & ~1;
-    vp_group_entry(v, false, x, y, ACC_ATOMIC, b0, b0 + mi, b0 + 2 * mi, A, ld, t, GS, g);
+    vp_operands(vp, e, A, x, y);
+    vp_run(v, 1, x, y, ACC_ATOMIC, b0, b0 + e.mi, b0 + 2 * e.mi, A, t, GS, g);
   }
   __syncthreads(); // the next class lays its slices over these
 }
 
-// Stage 0: huge row items, then the block, half, quad and warp classes.
-// Stage 1: huge tile items.  Counters: [0] row items, [1] block class,
-// [2] warp class, [3] tile items, [4] half class, [5] quad class.
-__global__ void __launch_bounds__(VP_THREADS, 2) kron_vplan_kernel(const __grid_constant__ VParams vp)
+// The huge queue, then the block, half, quad and warp classes.
+__global__ void __launch_bounds__(VP_THREADS, VP_MINB)
+    kron_vplan_kernel(const __grid_constant__ VParams vp)
 {
   extern __shared__ __align__(16) double smem[];
-  __shared__ int s_idx;
-  __shared__ int s_gidx[4];
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  __shared__ int s_idx, s_flag;
+  __shared__ int s_gidx[VP_WARPS];
+  const int tid = threadIdx.x;
   const double *A[6];
-  int ld[6];
   const double *x;
   double *y;
+  bool dead = false; // a chunk wait of this block gave up: skip later tile items
 
-  if (vp.stage == 1)
-  {
-    // ---- phase 2 of huge entries: head modes on column tiles -> y
-    while (true)
-    {
-      const int idx = block_take(&vp.counters[3], &s_idx, tid);
-      if (idx >= vp.ntile)
-        break;
-      const VItem it = vp.items[vp.nrow + idx];
-      const VDesc e  = vp.desc[it.d];
-      vp_operands(vp, e, A, ld, x, y);
-      const HugeDims hd = huge_dims(e);
-      const double *wr  = vp.ws + e.woff;
-      GenView v2;
-      vp_view(v2, e, 0, e.q);
-      v2.forward = e.fwd2;
-      v2.C       = e.C;
-      v2.in_row = v2.out_row = hd.Mtail;
-      const int mi2 = e.mi2;
-      for (int t = it.lo; t < it.hi; t++)
-      {
-        const int c0  = t * e.C;
-        v2.total_cols = min((int)e.C, hd.Mtail - c0);
-        vp_group_entry(v2, true, wr + c0, y + c0, ACC_ATOMIC, smem, smem + mi2, smem + 2 * mi2,
-                       A, ld, tid, VP_THREADS, 0);
-      }
-    }
-    return;
-  }
-
-  // ---- phase 1 of huge entries: tail modes on head rows -> the entry's region
   while (true)
   {
     const int idx = block_take(&vp.counters[0], &s_idx, tid);
-    if (idx >= vp.nrow)
+    if (idx >= vp.nitems)
       break;
     const VItem it = vp.items[idx];
-    const VDesc e  = vp.desc[it.d];
-    vp_operands(vp, e, A, ld, x, y);
+    const VDesc e  = vp.desc[it.e];
+    vp_operands(vp, e, A, x, y);
     const HugeDims hd = huge_dims(e);
     double *wr        = vp.ws + e.woff;
-    GenView v1;
-    vp_view(v1, e, e.q, e.d - e.q);
-    v1.forward    = e.fwd1;
-    const int mi1 = e.mi;
-    if (e.pad[0])
+    if (it.kind == 0)
     {
-      // one head row per warp (the plan checked that eight slices fit)
-      const int slice = (2 * mi1 + e.pad[1] * 16 + 1) & ~1;
-      double *b0      = smem + warp * slice;
-      // the warp's factors stay in its slice from its first row on
-      for (int h = it.lo + warp; h < it.hi; h += VP_WARPS)
-        vp_group_entry(v1, false, x + (long long)h * hd.Ntail, wr + (long long)h * hd.Mtail,
-                       ACC_STORE, b0, b0 + mi1, b0 + 2 * mi1, A, ld, lane, 32, warp,
-                       h == it.lo + warp);
+      // phase 1: tail modes on head rows [lo, hi) -> the entry's region
+      GenView v1;
+      vp_view(v1, e, e.q, e.d - e.q);
+      v1.forward = e.fwd1;
+      vp_run(v1, it.hi - it.lo, x + (long long)it.lo * hd.Ntail,
+             wr + (long long)it.lo * hd.Mtail, ACC_STORE, smem, smem + e.mi, smem + 2 * e.mi, A,
+             tid, VP_THREADS, 0);
+      // vp_run ended with a block barrier: every store of the chunk is issued
+      if (tid == 0)
+      {
+        __threadfence();
+        atomicAdd(vp.counters + NCOUNT + it.e, 1);
+      }
     }
     else
-      for (int h = it.lo; h < it.hi; h++)
-        vp_group_entry(v1, false, x + (long long)h * hd.Ntail, wr + (long long)h * hd.Mtail,
-                       ACC_STORE, smem, smem + mi1, smem + 2 * mi1, A, ld, tid, VP_THREADS, 0,
-                       h == it.lo);
-    __syncthreads();
+    {
+      // phase 2: head modes on column tile lo of the region -> y
+      if (!dead && !vp_wait_chunks(vp, it.e, e.nchunk, &s_flag, tid))
+        dead = true;
+      if (dead)
+        continue;
+      GenView v2;
+      vp_view(v2, e, 0, e.q);
+      v2.forward   = e.fwd2;
+      const int c0 = it.lo * e.C;
+      vp_run_tile(v2, wr + c0, hd.Mtail, e.C, min((int)e.C, hd.Mtail - c0), y + c0, hd.Mtail,
+                  smem, smem + e.mi2, smem + 2 * e.mi2, A, tid);
+    }
   }
 
-  // ---- block class: the whole block per entry
   const VDesc *blk = vp.desc + vp.nhuge;
-  while (true)
-  {
-    const int idx = block_take(&vp.counters[1], &s_idx, tid);
-    if (idx >= vp.nblock)
-      break;
-    const VDesc e = blk[idx];
-    GenView v;
-    vp_view(v, e, 0, e.d);
-    vp_operands(vp, e, A, ld, x, y);
-    const int mi = (e.mi + 1) & ~1;
-    vp_group_entry(v, false, x, y, ACC_ATOMIC, smem, smem + mi, smem + 2 * mi, A, ld, tid,
-                   VP_THREADS, 0);
-  }
-
-  // ---- half and quad classes: two / four entries per block at a time
-  {
-    const VDesc *hd = vp.desc + vp.nhuge + vp.nblock;
-    group_class<VP_THREADS / 2>(vp, hd, vp.nhalf, &vp.counters[4], smem, s_gidx, tid);
-    group_class<VP_THREADS / 4>(vp, hd + vp.nhalf, vp.nquad, &vp.counters[5], smem, s_gidx, tid);
-  }
-
-  // ---- warp class: one warp per entry
-  const int slice = vp.block_elems / VP_WARPS;
-  double *b0      = smem + warp * slice;
-  const VDesc *wd = vp.desc + vp.nhuge + vp.nblock + vp.nhalf + vp.nquad;
-  while (true)
-  {
-    int idx = 0;
-    if (lane == 0)
-      idx = atomicAdd(&vp.counters[2], 1);
-    idx = __shfl_sync(0xffffffffu, idx, 0);
-    if (idx >= vp.nwarp)
-      break;
-    const VDesc e = wd[idx];
-    GenView v;
-    vp_view(v, e, 0, e.d);
-    vp_operands(vp, e, A, ld, x, y);
-    vp_group_entry(v, false, x, y, ACC_ATOMIC, b0, b0 + WARP_MAX, b0 + 2 * WARP_MAX, A, ld, lane,
-                   32, warp);
-  }
+  group_class<VP_THREADS>(vp, blk, vp.nblock, &vp.counters[1], smem, s_gidx, tid);
+  blk += vp.nblock;
+  group_class<VP_THREADS / 2>(vp, blk, vp.nhalf, &vp.counters[4], smem, s_gidx, tid);
+  blk += vp.nhalf;
+  group_class<VP_THREADS / 4>(vp, blk, vp.nquad, &vp.counters[5], smem, s_gidx, tid);
+  blk += vp.nquad;
+  group_class<32>(vp, blk, vp.nwarp, &vp.counters[2], smem, s_gidx, tid);
 }
 
 } // namespace
@@ -341,19 +357,75 @@ struct kron_vplan_st
 {
   int batch;
   int nhuge, nblock, nhalf, nquad, nwarp;
-  int nrow, ntile;
+  int nitems;
   VDesc *d_desc;
   VItem *d_items;
-  int *d_counters;
+  int *d_counters;            // NCOUNT work counters + one chunk counter per huge entry
   double flops;
   size_t ws_bytes;
-  size_t smem_main, smem_huge, smem_tile;
-  int block_elems;
+  int budget;                 // shared elements per block
+  int grid_work;              // work units of the launch (grid upper bound)
   // graph cache
   cudaGraphExec_t exec;
   const void *gA, *gX, *gY, *gW;
   size_t gWcap;
 };
+
+namespace {
+
+long long even(long long v) { return (v + 1) & ~1LL; }
+
+// Two-phase split of a huge entry for a block of `budget` shared elements:
+// phase 1 applies modes [q, d) to chunks of R head rows, phase 2 modes
+// [0, q) to column tiles of C columns.  Prefers tiles of >= 16 columns
+// (128-byte row segments), then the smallest region (Nhead x Mtail).
+struct HugeSplit
+{
+  int q, C, R, fwd1, fwd2;
+  long long mi1, mi2; // buffer elements: per head row (phase 1), per column (phase 2)
+};
+
+bool plan_huge(int d, const int *m, const int *n, long long budget, HugeSplit &best)
+{
+  bool found = false;
+  long long best_w = 0;
+  int best_c = 0;
+  for (int q = 1; q < d; q++)
+  {
+    const bool f1    = choose_forward(d - q, m + q, n + q);
+    const bool f2    = choose_forward(q, m, n);
+    const long long r1 = max_intermediate(d - q, m + q, n + q, f1);
+    const long long r2 = max_intermediate(q, m, n, f2);
+    long long a1 = 0, a2 = 0, Nhead = 1, Mtail = 1;
+    for (int l = 0; l < q; l++)
+    {
+      a2 += (long long)m[l] * n[l];
+      Nhead *= n[l];
+    }
+    for (int l = q; l < d; l++)
+    {
+      a1 += (long long)m[l] * n[l];
+      Mtail *= m[l];
+    }
+    const long long R = (budget - even(a1) - 2) / (2 * r1);
+    const long long C = std::min<long long>({255, Mtail, (budget - even(a2) - 2) / (2 * r2)});
+    if (R < 1 || C < 1)
+      continue;
+    const int cq        = (int)std::min<long long>(C, 16);
+    const long long wsz = Nhead * Mtail;
+    if (!found || cq > best_c || (cq == best_c && wsz < best_w))
+    {
+      best = HugeSplit{q, (int)C, (int)std::min<long long>(R, 65535), f1 ? 1 : 0, f2 ? 1 : 0,
+                       r1, r2};
+      best_c = cq;
+      best_w = wsz;
+      found  = true;
+    }
+  }
+  return found;
+}
+
+} // namespace
 
 extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const shapes[])
 {
@@ -361,14 +433,13 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
     return KRON_ERROR_INVALID_VALUE;
   *plan = nullptr;
   const DeviceInfo &di = device_info();
-  const int maxsm      = di.max_smem_optin;
-  // block class: two buffers + factors within the block's shared memory
-  const int block_elems = (maxsm - 4096) / 8;
+  // shared elements per block: two blocks per SM (1 KB of each block's share
+  // is reserved by the hardware, and the kernel's own variables)
+  const long long budget =
+      (std::min<long long>(di.max_smem_optin, di.smem_per_sm / VP_MINB - 1024) - 256) / 8 & ~1LL;
   std::vector<VDesc> cls[NCLS];
   std::vector<double> cost[NCLS];
-  double total_flops   = 0.0;
-  size_t smem_huge     = 0;
-  size_t smem_tile     = 0;
+  double total_flops = 0.0;
   for (int k = 0; k < batchCount; k++)
   {
     const int *s = shapes + 13LL * k;
@@ -391,63 +462,45 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
     e.d              = (unsigned char)d;
     const bool fwd   = choose_forward(d, m, n);
     e.fwd            = fwd ? 1 : 0;
-    const long long mi = max_intermediate(d, m, n, fwd);
+    const long long mi = even(max_intermediate(d, m, n, fwd));
     const double fl  = std::min(flops_forward(d, m, n), flops_backward(d, m, n));
     total_flops += fl;
     long long asz = 0;
     for (int l = 0; l < d; l++)
       asz += (long long)m[l] * n[l];
-    const long long mi2r = (mi + 1) & ~1LL;
+    const long long need = 2 * mi + even(asz);
     int c;
-    const long long need = 2 * mi2r + asz;
-    if (mi <= WARP_MAX && 2 * WARP_MAX + asz <= block_elems / VP_WARPS)
+    if (mi <= WARP_MAX && 2 * WARP_MAX + even(asz) <= (budget / VP_WARPS & ~1LL))
       c = CLS_WARP;
-    else if (need <= ((block_elems / 4) & ~1))
+    else if (need <= (budget / 4 & ~1LL))
       c = CLS_QUAD;
-    else if (need <= ((block_elems / 2) & ~1))
+    else if (need <= (budget / 2 & ~1LL))
       c = CLS_HALF;
-    else if (need <= block_elems)
+    else if (need <= budget)
       c = CLS_BLOCK;
     else
     {
       c = CLS_HUGE;
-      LargePlan lp;
-      if (!plan_large(d, m, n, 8, false, lp) || lp.C > 255)
+      HugeSplit hs;
+      if (!plan_huge(d, m, n, budget, hs))
         return KRON_ERROR_NOT_SUPPORTED;
-      e.q    = (unsigned char)lp.q;
-      e.fwd1 = (unsigned char)lp.v1.forward;
-      e.fwd2 = (unsigned char)lp.v2.forward;
-      // phase-2 tiles narrowed so that one fits half the shared memory (two
-      // blocks per SM run the tile launch)
-      {
-        const long long rows2 = std::max<long long>(1, lp.v2.max_inter / std::max(1, lp.C));
-        const long long budget = (long long)(maxsm / 2 - 1024) / 8 - lp.v2.asz;
-        long long C2 = std::min<long long>(lp.C, budget / (2 * rows2));
-        if (C2 < 1)
-          C2 = lp.C; // keep the plan's width; the tile launch then runs one block per SM
-        e.C   = (unsigned char)C2;
-        e.mi2 = (int)((rows2 * C2 + 1) & ~1LL);
-        smem_tile = std::max(smem_tile, (size_t)(2 * e.mi2 + lp.v2.asz + 2) * 8);
-      }
-      size_t need = (size_t)std::max(lp.v1.group_elems, lp.v2.group_elems) * 8;
-      // phase 1 one block per warp when eight slices fit
-      const long long a16   = (lp.v1.asz + 15) / 16;
-      const long long slice = (2LL * lp.v1.max_inter + a16 * 16 + 1) & ~1LL;
-      if (a16 < 256 && (size_t)(VP_WARPS * slice * 8) <= (size_t)(maxsm - 1024))
-      {
-        e.pad[0] = 1;
-        e.pad[1] = (unsigned char)a16;
-        need     = std::max(need, (size_t)(VP_WARPS * slice * 8));
-      }
-      smem_huge = std::max(smem_huge, need);
+      e.q    = (unsigned char)hs.q;
+      e.C    = (unsigned char)hs.C;
+      e.fwd1 = (unsigned char)hs.fwd1;
+      e.fwd2 = (unsigned char)hs.fwd2;
+      long long Nhead = 1;
+      for (int l = 0; l < hs.q; l++)
+        Nhead *= n[l];
+      // chunks of equal size, at most R rows each
+      const long long nchunk = (Nhead + hs.R - 1) / hs.R;
+      const long long R      = (Nhead + nchunk - 1) / nchunk;
+      e.R      = (unsigned short)R;
+      e.nchunk = (int)nchunk;
+      e.mi     = (int)even(R * hs.mi1);
+      e.mi2    = (int)even(hs.C * hs.mi2);
     }
-    e.mi = (c == CLS_HUGE) ? 0 : (int)mi;
-    if (c == CLS_HUGE)
-    {
-      LargePlan lp;
-      plan_large(d, m, n, 8, false, lp);
-      e.mi = lp.v1.max_inter; // phase-1 buffer elements, rounded
-    }
+    if (c != CLS_HUGE)
+      e.mi = (c == CLS_WARP) ? WARP_MAX : (int)mi;
     cls[c].push_back(e);
     cost[c].push_back(fl);
   }
@@ -472,71 +525,69 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
   pl->nquad  = (int)cls[CLS_QUAD].size();
   pl->nwarp  = (int)cls[CLS_WARP].size();
 
-  // workspace regions and work items of the huge entries: row items of
-  // about 32k input elements (whole warps' worth of rows), tile items of one
-  // column tile; each list largest first
-  std::vector<VItem> rows, tiles;
-  std::vector<double> rcost, tcost;
-  long long woff = 0;
+  // The huge queue: entries largest first; an entry's tile items enter the
+  // queue once `lag_items` items or `lag_elems` elements of live regions
+  // separate them from its chunk items (whichever comes first), so a tile
+  // item rarely waits and its region is still in L2.  Regions start on
+  // 128-byte boundaries.
+  std::vector<VItem> items;
+  const long long lag_items = 2LL * di.sms * VP_MINB;
+  const long long lag_elems = 40LL << 17; // 40 MB of regions
+  struct Pending
+  {
+    int e;
+    size_t pos;
+    long long elems;
+  };
+  std::vector<Pending> pend;
+  size_t pend_head   = 0;
+  long long live     = 0;
+  long long woff     = 0;
+  auto emit_tiles = [&](const Pending &p) {
+    const VDesc &e = all[p.e];
+    long long Mtail = 1;
+    for (int l = e.q; l < e.d; l++)
+      Mtail *= e.m[l];
+    const long long nt = (Mtail + e.C - 1) / e.C;
+    for (long long t = 0; t < nt; t++)
+      items.push_back(VItem{p.e, (int)t, (int)t + 1, 1});
+    live -= p.elems;
+  };
   for (int i = 0; i < pl->nhuge; i++)
   {
     VDesc &e = all[i];
     e.woff   = woff;
-    long long Nhead = 1, Ntail = 1, Mtail = 1, Mhead = 1;
+    long long Nhead = 1, Mtail = 1;
     for (int l = 0; l < e.q; l++)
-    {
       Nhead *= e.n[l];
-      Mhead *= e.m[l];
-    }
     for (int l = e.q; l < e.d; l++)
-    {
-      Ntail *= e.n[l];
       Mtail *= e.m[l];
-    }
-    woff += (Nhead * Mtail + 1) & ~1LL;
-    long long rpi = std::max<long long>(1, 32768 / std::max<long long>(1, Ntail));
-    rpi           = std::max<long long>(VP_WARPS, (rpi + VP_WARPS - 1) / VP_WARPS * VP_WARPS);
-    for (long long h0 = 0; h0 < Nhead; h0 += rpi)
-    {
-      const long long h1 = std::min(Nhead, h0 + rpi);
-      rows.push_back(VItem{i, (int)h0, (int)h1, 0});
-      rcost.push_back((double)(h1 - h0) * (double)(Ntail + Mtail));
-    }
-    const long long nt = (Mtail + e.C - 1) / e.C;
-    for (long long t = 0; t < nt; t++)
-    {
-      tiles.push_back(VItem{i, (int)t, (int)t + 1, 0});
-      tcost.push_back((double)std::min<long long>(e.C, Mtail - t * e.C) * (double)(Nhead + Mhead));
-    }
+    const long long region = (Nhead * Mtail + 15) & ~15LL;
+    woff += region;
+    for (long long h0 = 0; h0 < Nhead; h0 += e.R)
+      items.push_back(VItem{i, (int)h0, (int)std::min<long long>(Nhead, h0 + e.R), 0});
+    pend.push_back(Pending{i, items.size(), region});
+    live += region;
+    while (pend_head < pend.size() &&
+           ((long long)(items.size() - pend[pend_head].pos) >= lag_items || live > lag_elems))
+      emit_tiles(pend[pend_head++]);
   }
-  auto sorted = [](std::vector<VItem> &v, const std::vector<double> &c) {
-    std::vector<int> o(v.size());
-    std::iota(o.begin(), o.end(), 0);
-    std::stable_sort(o.begin(), o.end(), [&](int a, int b) { return c[a] > c[b]; });
-    std::vector<VItem> r;
-    r.reserve(v.size());
-    for (int i : o)
-      r.push_back(v[i]);
-    return r;
-  };
-  std::vector<VItem> items = sorted(rows, rcost);
-  {
-    std::vector<VItem> t = sorted(tiles, tcost);
-    items.insert(items.end(), t.begin(), t.end());
-  }
-  pl->nrow        = (int)rows.size();
-  pl->ntile       = (int)tiles.size();
-  pl->flops       = total_flops;
-  pl->block_elems = block_elems;
-  pl->smem_main   = (size_t)block_elems * 8;
-  pl->smem_huge   = std::max<size_t>(smem_huge, 16);
-  pl->smem_tile   = std::max<size_t>(smem_tile, 16);
-  pl->ws_bytes    = (size_t)woff * 8;
-  pl->exec        = nullptr;
-  pl->d_desc      = nullptr;
-  pl->d_items     = nullptr;
-  pl->d_counters  = nullptr;
-  if (kron::dev_malloc((void **)&pl->d_counters, 8 * sizeof(int)) != cudaSuccess ||
+  while (pend_head < pend.size())
+    emit_tiles(pend[pend_head++]);
+
+  pl->nitems     = (int)items.size();
+  pl->flops      = total_flops;
+  pl->budget     = (int)budget;
+  pl->ws_bytes   = (size_t)woff * 8;
+  pl->grid_work  = (int)std::min<long long>(
+      1LL << 30, (long long)items.size() + pl->nblock + (pl->nhalf + 1) / 2 +
+                     (pl->nquad + 3) / 4 + (pl->nwarp + VP_WARPS - 1) / VP_WARPS);
+  pl->exec       = nullptr;
+  pl->d_desc     = nullptr;
+  pl->d_items    = nullptr;
+  pl->d_counters = nullptr;
+  const size_t ncount = NCOUNT + (size_t)pl->nhuge;
+  if (kron::dev_malloc((void **)&pl->d_counters, ncount * sizeof(int)) != cudaSuccess ||
       (batchCount > 0 && kron::dev_malloc((void **)&pl->d_desc, sizeof(VDesc) * batchCount) != cudaSuccess) ||
       (!items.empty() && kron::dev_malloc((void **)&pl->d_items, sizeof(VItem) * items.size()) != cudaSuccess))
   {
@@ -580,55 +631,43 @@ extern "C" double kron_vplan_flops(kron_vplan_t plan) { return plan ? plan->flop
 static int vplan_launch_all(kron_vplan_t pl, double const *const *A, double **X, double **Y,
                             void *W, cudaStream_t s)
 {
-  if (cudaMemsetAsync(pl->d_counters, 0, 8 * sizeof(int), s) != cudaSuccess)
+  if (cudaMemsetAsync(pl->d_counters, 0, (NCOUNT + (size_t)pl->nhuge) * sizeof(int), s) !=
+      cudaSuccess)
     return KRON_ERROR_LAUNCH;
+  if (pl->grid_work <= 0)
+    return KRON_SUCCESS;
   VParams vp;
   std::memset(&vp, 0, sizeof(vp));
-  vp.desc        = pl->d_desc;
-  vp.items       = pl->d_items;
-  vp.nhuge       = pl->nhuge;
-  vp.nblock      = pl->nblock;
-  vp.nhalf       = pl->nhalf;
-  vp.nquad       = pl->nquad;
-  vp.nwarp       = pl->nwarp;
-  vp.nrow        = pl->nrow;
-  vp.ntile       = pl->ntile;
-  vp.counters    = pl->d_counters;
-  vp.pA          = A;
-  vp.pX          = X;
-  vp.pY          = Y;
-  vp.ws          = static_cast<double *>(W);
-  vp.block_elems = pl->block_elems;
-  void *args[]   = {&vp};
-  const int sms  = device_info().sms;
-  const void *fm = reinterpret_cast<const void *>(&kron_vplan_kernel);
-  const size_t smem = std::max(pl->smem_main, pl->smem_huge);
+  vp.desc     = pl->d_desc;
+  vp.items    = pl->d_items;
+  vp.nhuge    = pl->nhuge;
+  vp.nblock   = pl->nblock;
+  vp.nhalf    = pl->nhalf;
+  vp.nquad    = pl->nquad;
+  vp.nwarp    = pl->nwarp;
+  vp.nitems   = pl->nitems;
+  vp.counters = pl->d_counters;
+  vp.status   = device_status_ptr();
+  vp.spin     = wait_limit();
+  vp.pA       = A;
+  vp.pX       = X;
+  vp.pY       = Y;
+  vp.ws       = static_cast<double *>(W);
+  vp.budget   = pl->budget;
+  void *args[]      = {&vp};
+  const void *fm    = reinterpret_cast<const void *>(&kron_vplan_kernel);
+  const size_t smem = (size_t)pl->budget * 8;
   int occ           = 1;
   if (cached_occupancy(fm, VP_THREADS, smem, &occ) != KRON_SUCCESS)
     return KRON_ERROR_LAUNCH;
-  const long long work0 = (long long)pl->nrow + pl->nblock + (pl->nhalf + 1) / 2 +
-                          (pl->nquad + 3) / 4 + (pl->nwarp + VP_WARPS - 1) / VP_WARPS;
-  if (work0 > 0)
-  {
-    vp.stage       = 0;
-    const int grid = (int)std::max<long long>(1, std::min<long long>((long long)sms * occ, work0));
-    if (cudaLaunchKernel(fm, dim3(grid), dim3(VP_THREADS), args, smem, s) != cudaSuccess)
-      return KRON_ERROR_LAUNCH;
-  }
-  if (pl->ntile > 0)
-  {
-    vp.stage   = 1;
-    int occ1   = 1;
-    if (cached_occupancy(fm, VP_THREADS, pl->smem_tile, &occ1) != KRON_SUCCESS)
-      return KRON_ERROR_LAUNCH;
-    const int grid = std::max(1, std::min(sms * occ1, pl->ntile));
-    if (cudaLaunchKernel(fm, dim3(grid), dim3(VP_THREADS), args, pl->smem_tile, s) !=
-        cudaSuccess)
-      return KRON_ERROR_LAUNCH;
-  }
+  // persistent: every block stays resident until the queues run dry
+  const int grid =
+      (int)std::max<long long>(1, std::min<long long>((long long)device_info().sms * occ,
+                                                      pl->grid_work));
+  if (cudaLaunchKernel(fm, dim3(grid), dim3(VP_THREADS), args, smem, s) != cudaSuccess)
+    return KRON_ERROR_LAUNCH;
   return KRON_SUCCESS;
 }
-
 extern "C" int kron_vplan_execute_async(kron_vplan_t plan, double const *const Aarray_[],
                                         double *pX_[], double *pY_[], void *W,
                                         size_t Wcapacity_bytes, kron_stream_t stream)
