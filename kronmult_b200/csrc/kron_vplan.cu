@@ -50,6 +50,7 @@ constexpr int NCOUNT = 8;         // work counters ahead of the per-entry chunk 
 
 struct VDesc
 {
+  // fetched as twelve 32-bit words by the kernel's fetch stages
   long long woff;       // huge: element offset of the entry's workspace region
   int k;                // entry index (operands at pA[6k + l], pX[k], pY[k])
   unsigned char d, fwd, q, C;  // order; huge: head modes q, tile columns C
@@ -61,6 +62,8 @@ struct VDesc
   unsigned short R;           // huge: head rows per chunk item
   int nchunk;                 // huge: chunk items (its tile items wait for all)
 };
+
+static_assert(sizeof(VDesc) == 48, "VDesc is fetched as 12 words");
 
 // kind 0: chunk item, head rows [lo, hi); kind 1: tile item, column tile lo
 // of the huge entry desc[e]
@@ -122,9 +125,14 @@ __device__ __forceinline__ void vp_load_factors(const GenView &v, double *As,
 // rows consecutive vectors of the view (x contiguous) computed by a group
 // of GS threads in buffers b0 / b1 (each >= rows x the largest
 // intermediate), factors at As; the results go to out (contiguous).
+// hook(s) runs the next item's fetch stage s at four points: after the
+// copies are issued, after they land, before the results go out, and
+// before the closing barrier.
+template <typename Hook>
 __device__ __forceinline__ void vp_run(const GenView &v, int rows, const double *x, double *out,
                                        int accum, double *b0, double *b1, double *As,
-                                       const double *const *A, int t, int GS, int g)
+                                       const double *const *A, int t, int GS, int g,
+                                       const Hook &hook)
 {
   vp_load_factors(v, As, A, t, GS);
   int rin = rows, rout = rows;
@@ -135,21 +143,27 @@ __device__ __forceinline__ void vp_run(const GenView &v, int rows, const double 
   }
   for (int i = t; i < rin; i += GS)
     cp8(b0 + i, x + i);
+  hook(1);
   cp_wait_all();
   group_sync(g, GS);
+  hook(2);
   double *cur = b0, *nxt = b1;
   gen_apply_modes<double, PREC_F64, true>(v, cur, nxt, As, 1, t, GS, g, rows);
+  hook(3);
   group_flush(accum, out, cur, cur, false, rout, t, GS);
+  hook(4);
   group_sync(g, GS);
 }
 
 // One column tile of a huge entry's region: rows of C columns at stride
 // in_row (the first Cc valid, the rest zero-filled), the head modes, and
-// the Cc valid columns added into y (row stride out_row).  Whole block.
+// the Cc valid columns added into y (row stride out_row).  Whole block;
+// hook as for vp_run.
+template <typename Hook>
 __device__ __forceinline__ void vp_run_tile(const GenView &v, const double *w, long long in_row,
                                             int C, int Cc, double *y, long long out_row,
                                             double *b0, double *b1, double *As,
-                                            const double *const *A, int tid)
+                                            const double *const *A, int tid, const Hook &hook)
 {
   vp_load_factors(v, As, A, tid, VP_THREADS);
   int rin = 1, rout = 1;
@@ -162,14 +176,126 @@ __device__ __forceinline__ void vp_run_tile(const GenView &v, const double *w, l
   for (int h = warp; h < rin; h += VP_WARPS)
     for (int c = lane; c < C; c += 32)
       cp8(b0 + h * C + c, w + h * in_row + (c < Cc ? c : 0), c < Cc);
+  hook(1);
   cp_wait_all();
   __syncthreads();
+  hook(2);
   double *cur = b0, *nxt = b1;
   gen_apply_modes<double, PREC_F64, true>(v, cur, nxt, As, C, tid, VP_THREADS, 0);
+  hook(3);
   for (int i = warp; i < rout; i += VP_WARPS)
     for (int c = lane; c < Cc; c += 32)
       red_add(y + i * out_row + c, cur[i * C + c]);
+  hook(4);
   __syncthreads();
+}
+
+// What a group needs to start its next item, in shared memory.  The
+// group's first warp fetches it in stages during the current item, one
+// dependent load per stage (queue index, item, descriptor, operand
+// pointers), so none of those round trips stalls the group.
+struct NextSlot
+{
+  int idx;               // queue / list position (>= the count: no more work)
+  int ready;             // huge tile item: its entry's chunks were complete
+  VItem it;              // huge queue only
+  VDesc e;
+  const double *ptr[8];  // A_1..A_6, x, y
+};
+
+// The fetching warp's registers between stages.
+struct Fetch
+{
+  int r;                 // lane 0: the counter's old value; lanes: a word in flight
+  int nidx;
+  const double *p;       // lanes 0-7: a pointer in flight
+};
+
+// Stages of the fetch for the huge queue (kind = true) or a class list.
+// Stage 0 takes the next position; 1 loads the item (huge) or the
+// descriptor; 2 stores it and loads the descriptor (huge) or the pointers;
+// 3 and 4 finish.  Every store to the slot happens after the current item
+// has read the slot (the first barrier of the item lies between).
+template <bool HUGE>
+__device__ __forceinline__ void fetch_stage(int s, Fetch &f, NextSlot &slot, const VParams &vp,
+                                            const VDesc *list, int n, int *counter, int lane)
+{
+  const unsigned FULL = 0xffffffffu;
+  if (s == 0)
+  {
+    if (lane == 0)
+      f.r = atomicAdd(counter, 1);
+    return;
+  }
+  if (s == 1)
+  {
+    f.nidx = __shfl_sync(FULL, f.r, 0);
+    if (f.nidx < n)
+    {
+      if (HUGE && lane < 4)
+        f.r = reinterpret_cast<const int *>(vp.items + f.nidx)[lane];
+      if (!HUGE && lane < 12)
+        f.r = reinterpret_cast<const int *>(list + f.nidx)[lane];
+    }
+    return;
+  }
+  const bool more = f.nidx < n;
+  if (HUGE)
+  {
+    if (s == 2)
+    {
+      if (lane == 0)
+        slot.idx = f.nidx;
+      if (more && lane < 4)
+        reinterpret_cast<int *>(&slot.it)[lane] = f.r;
+      __syncwarp();
+      if (more && lane < 12)
+        f.r = reinterpret_cast<const int *>(vp.desc + slot.it.e)[lane];
+    }
+    else if (s == 3)
+    {
+      if (more && lane < 12)
+        reinterpret_cast<int *>(&slot.e)[lane] = f.r;
+      __syncwarp();
+      if (more && lane < 8)
+      {
+        const int k = slot.e.k, d = slot.e.d;
+        f.p = lane < 6 ? (lane < d ? vp.pA[6LL * k + lane] : nullptr)
+                       : (lane == 6 ? vp.pX[k] : vp.pY[k]);
+      }
+      if (more && lane == 8)
+        f.r = slot.it.kind == 1 && ld_acquire(vp.counters + NCOUNT + slot.it.e) >= slot.e.nchunk;
+    }
+    else
+    {
+      if (more && lane < 8)
+        slot.ptr[lane] = f.p;
+      if (more && lane == 8)
+        slot.ready = f.r;
+    }
+  }
+  else
+  {
+    if (s == 2)
+    {
+      if (lane == 0)
+        slot.idx = f.nidx;
+      if (more && lane < 12)
+        reinterpret_cast<int *>(&slot.e)[lane] = f.r;
+      __syncwarp();
+      if (more && lane < 8)
+      {
+        const int k = slot.e.k, d = slot.e.d;
+        f.p = lane < 6 ? (lane < d ? vp.pA[6LL * k + lane] : nullptr)
+                       : (lane == 6 ? vp.pX[k] : vp.pY[k]);
+      }
+    }
+    else if (s == 3)
+    {
+      if (more && lane < 8)
+        slot.ptr[lane] = f.p;
+    }
+  }
 }
 
 __device__ __forceinline__ void vp_view(GenView &v, const VDesc &e, int mode0, int dd)
@@ -185,15 +311,6 @@ __device__ __forceinline__ void vp_view(GenView &v, const VDesc &e, int mode0, i
   v.C       = 1;
   v.in_row = v.out_row = 1;
   v.total_cols         = 1;
-}
-
-__device__ __forceinline__ void vp_operands(const VParams &vp, const VDesc &e, const double *A[6],
-                                            const double *&x, double *&y)
-{
-  for (int l = 0; l < 6; l++)
-    A[l] = l < e.d ? vp.pA[6LL * e.k + l] : nullptr;
-  x = vp.pX[e.k];
-  y = vp.pY[e.k];
 }
 
 // Sizes of a huge entry's split: head inputs Nhead, tail inputs / outputs
@@ -214,17 +331,6 @@ __device__ __forceinline__ HugeDims huge_dims(const VDesc &e)
     h.Mtail *= e.m[l];
   }
   return h;
-}
-
-// next work item of a list for the whole block
-__device__ __forceinline__ int block_take(int *counter, int *s_idx, int tid)
-{
-  if (tid == 0)
-    *s_idx = atomicAdd(counter, 1);
-  __syncthreads();
-  const int idx = *s_idx;
-  __syncthreads();
-  return idx;
 }
 
 // Thread 0 polls the entry's chunk counter (acquire) until `need` chunk
@@ -256,34 +362,56 @@ __device__ __forceinline__ bool vp_wait_chunks(const VParams &vp, int e, int nee
   return *s_flag != 0;
 }
 
+// Read the slot into the item's registers (every thread of the group).
+__device__ __forceinline__ void slot_read(const NextSlot &slot, VDesc &e, const double *A[6],
+                                          const double *&x, double *&y)
+{
+  e = slot.e;
+  for (int l = 0; l < 6; l++)
+    A[l] = slot.ptr[l];
+  x = slot.ptr[6];
+  y = const_cast<double *>(slot.ptr[7]);
+}
+
 // Entries of one class run by groups of GS threads, VP_THREADS / GS per
-// block, each group with its own slice of shared memory and barrier.
+// block, each group with its own slice of shared memory, barrier and slot.
 template <int GS>
 __device__ __forceinline__ void group_class(const VParams &vp, const VDesc *list, int n,
-                                            int *counter, double *smem, int *s_gidx, int tid)
+                                            int *counter, double *smem, NextSlot *slots, int tid)
 {
   constexpr int NG = VP_THREADS / GS;
-  const int g = tid / GS, t = tid - (tid / GS) * GS;
-  double *b0  = smem + (long long)g * ((vp.budget / NG) & ~1);
+  const int g = tid / GS, t = tid - (tid / GS) * GS, lane = tid & 31;
+  double *b0     = smem + (long long)g * ((vp.budget / NG) & ~1);
+  NextSlot &slot = slots[g];
+  const bool fw  = t < 32; // the group's first warp fetches
+  Fetch f{0, 0, nullptr};
+  if (fw)
+    for (int st = 0; st < 4; st++)
+    {
+      fetch_stage<false>(st, f, slot, vp, list, n, counter, lane);
+      __syncwarp();
+    }
+  group_sync(g, GS);
   const double *A[6];
   const double *x;
   double *y;
+  VDesc e;
   while (true)
   {
-    if (t == 0)
-      s_gidx[g] = atomicAdd(counter, 1);
-    group_sync(g, GS);
-    const int idx = s_gidx[g];
-    group_sync(g, GS);
+    const int idx = slot.idx;
     if (idx >= n)
       break;
-    const VDesc e = list[idx];
+    slot_read(slot, e, A, x, y);
+    if (fw)
+      fetch_stage<false>(0, f, slot, vp, list, n, counter, lane);
     GenView v;
     vp_view(v, e, 0, e.d);
-    vp_operands(vp, e, A, x, y);
-    vp_run(v, 1, x, y, ACC_ATOMIC, b0, b0 + e.mi, b0 + 2 * e.mi, A, t, GS, g);
+    vp_run(v, 1, x, y, ACC_ATOMIC, b0, b0 + e.mi, b0 + 2 * e.mi, A, t, GS, g, [&](int st) {
+      if (fw && st < 4)
+        fetch_stage<false>(st, f, slot, vp, list, n, counter, lane);
+    });
   }
-  __syncthreads(); // the next class lays its slices over these
+  __syncthreads(); // the next class lays its slices (and slots) over these
 }
 
 // The huge queue, then the block, half, quad and warp classes.
@@ -291,22 +419,38 @@ __global__ void __launch_bounds__(VP_THREADS, VP_MINB)
     kron_vplan_kernel(const __grid_constant__ VParams vp)
 {
   extern __shared__ __align__(16) double smem[];
-  __shared__ int s_idx, s_flag;
-  __shared__ int s_gidx[VP_WARPS];
-  const int tid = threadIdx.x;
+  __shared__ int s_flag;
+  __shared__ NextSlot s_slot[VP_WARPS];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const bool fw = tid < 32;
   const double *A[6];
   const double *x;
   double *y;
+  VDesc e;
   bool dead = false; // a chunk wait of this block gave up: skip later tile items
 
+  NextSlot &slot = s_slot[0];
+  Fetch f{0, 0, nullptr};
+  if (fw)
+    for (int st = 0; st < 5; st++)
+    {
+      fetch_stage<true>(st, f, slot, vp, nullptr, vp.nitems, &vp.counters[0], lane);
+      __syncwarp();
+    }
+  __syncthreads();
+  auto hook = [&](int st) {
+    if (fw)
+      fetch_stage<true>(st, f, slot, vp, nullptr, vp.nitems, &vp.counters[0], lane);
+  };
   while (true)
   {
-    const int idx = block_take(&vp.counters[0], &s_idx, tid);
-    if (idx >= vp.nitems)
+    if (slot.idx >= vp.nitems)
       break;
-    const VItem it = vp.items[idx];
-    const VDesc e  = vp.desc[it.e];
-    vp_operands(vp, e, A, x, y);
+    const VItem it   = slot.it;
+    const bool ready = slot.ready != 0;
+    slot_read(slot, e, A, x, y);
+    if (fw)
+      fetch_stage<true>(0, f, slot, vp, nullptr, vp.nitems, &vp.counters[0], lane);
     const HugeDims hd = huge_dims(e);
     double *wr        = vp.ws + e.woff;
     if (it.kind == 0)
@@ -317,7 +461,7 @@ __global__ void __launch_bounds__(VP_THREADS, VP_MINB)
       v1.forward = e.fwd1;
       vp_run(v1, it.hi - it.lo, x + (long long)it.lo * hd.Ntail,
              wr + (long long)it.lo * hd.Mtail, ACC_STORE, smem, smem + e.mi, smem + 2 * e.mi, A,
-             tid, VP_THREADS, 0);
+             tid, VP_THREADS, 0, hook);
       // vp_run ended with a block barrier: every store of the chunk is issued
       if (tid == 0)
       {
@@ -328,27 +472,36 @@ __global__ void __launch_bounds__(VP_THREADS, VP_MINB)
     else
     {
       // phase 2: head modes on column tile lo of the region -> y
-      if (!dead && !vp_wait_chunks(vp, it.e, e.nchunk, &s_flag, tid))
+      if (!ready && !dead && !vp_wait_chunks(vp, it.e, e.nchunk, &s_flag, tid))
         dead = true;
       if (dead)
+      {
+        // keep the fetch going: the stages still run, the tile does not
+        for (int st = 1; st < 5; st++)
+        {
+          hook(st);
+          __syncthreads();
+        }
         continue;
+      }
       GenView v2;
       vp_view(v2, e, 0, e.q);
       v2.forward   = e.fwd2;
       const int c0 = it.lo * e.C;
       vp_run_tile(v2, wr + c0, hd.Mtail, e.C, min((int)e.C, hd.Mtail - c0), y + c0, hd.Mtail,
-                  smem, smem + e.mi2, smem + 2 * e.mi2, A, tid);
+                  smem, smem + e.mi2, smem + 2 * e.mi2, A, tid, hook);
     }
   }
+  __syncthreads();
 
   const VDesc *blk = vp.desc + vp.nhuge;
-  group_class<VP_THREADS>(vp, blk, vp.nblock, &vp.counters[1], smem, s_gidx, tid);
+  group_class<VP_THREADS>(vp, blk, vp.nblock, &vp.counters[1], smem, s_slot, tid);
   blk += vp.nblock;
-  group_class<VP_THREADS / 2>(vp, blk, vp.nhalf, &vp.counters[4], smem, s_gidx, tid);
+  group_class<VP_THREADS / 2>(vp, blk, vp.nhalf, &vp.counters[4], smem, s_slot, tid);
   blk += vp.nhalf;
-  group_class<VP_THREADS / 4>(vp, blk, vp.nquad, &vp.counters[5], smem, s_gidx, tid);
+  group_class<VP_THREADS / 4>(vp, blk, vp.nquad, &vp.counters[5], smem, s_slot, tid);
   blk += vp.nquad;
-  group_class<32>(vp, blk, vp.nwarp, &vp.counters[2], smem, s_gidx, tid);
+  group_class<32>(vp, blk, vp.nwarp, &vp.counters[2], smem, s_slot, tid);
 }
 
 } // namespace
@@ -434,9 +587,9 @@ extern "C" int kron_vplan_create(kron_vplan_t *plan, int batchCount, int const s
   *plan = nullptr;
   const DeviceInfo &di = device_info();
   // shared elements per block: two blocks per SM (1 KB of each block's share
-  // is reserved by the hardware, and the kernel's own variables)
+  // is reserved by the hardware; 2 KB cover the kernel's own variables)
   const long long budget =
-      (std::min<long long>(di.max_smem_optin, di.smem_per_sm / VP_MINB - 1024) - 256) / 8 & ~1LL;
+      (std::min<long long>(di.max_smem_optin, di.smem_per_sm / VP_MINB - 1024) - 2048) / 8 & ~1LL;
   std::vector<VDesc> cls[NCLS];
   std::vector<double> cost[NCLS];
   double total_flops = 0.0;
