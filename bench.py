@@ -529,7 +529,7 @@ class UnevenBatch(Workload):
         self.hYout = torch.empty_like(self.h["Y"]).pin_memory()
         self.h2d_bytes = sum(v.numel() * v.element_size() for v in self.h.values())
         self.d2h_bytes = self.hYout.numel() * 8
-        self.launches_per_step = 2
+        self.launches_per_step = 1  # one persistent kernel (after a counter memset)
 
     def step(self):
         self.plan.execute(self.pA, self.pX, self.pY, self.dW)
@@ -881,8 +881,8 @@ class KgemmBatched(Workload):
 
 def make_workload(cfg, precision, entries=0, n=6):
     """The workload of --config cfg (n: config 3's size); entries > 0 scales
-    its batch down (or up) for small profiling cases (configs 1, 3 and 5;
-    outputs of config 5 keep their 716:1024 ratio)."""
+    its batch down (or up) for small profiling cases (configs 1, 3, 4, 5
+    and 6; outputs of config 5 keep their 716:1024 ratio)."""
     if cfg == 1:
         return BatchedSquare(6, 4, entries or 512, "f64", "uniform")
     if cfg == 2:
@@ -890,7 +890,7 @@ def make_workload(cfg, precision, entries=0, n=6):
     if cfg == 3:
         return BatchedSquare(6, n, entries or 4096, precision, "normal", sweep=not entries)
     if cfg == 4:
-        return UnevenBatch()
+        return UnevenBatch(nent=entries or 20000)
     if cfg == 5:
         if entries:
             return XbatchedBig(batch=entries, nout=max(1, entries * 716 // 1024))

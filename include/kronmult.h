@@ -320,6 +320,26 @@ int kron_build_pointers_async(int d, int batchCount, double const *A, long long 
                               double *Xarray_out[], double *Yarray_out[], kron_stream_t stream);
 
 /* ------------------------------------------------------------------------
+ * Owner-computes sharding over several GPUs (no reference counterpart: the
+ * reference runs one device).  Host function, no GPU needed.  Outputs of an
+ * xbatched / pbatched batch may alias (ylist[k] == ylist[k'] for entries
+ * that add into one column); kron_owner_partition gives every output index
+ * to exactly one of nranks ranks, with every entry that writes it, so each
+ * rank finishes its outputs alone and no partial sums cross GPUs:
+ *   rank r owns outputs [out_bounds[r], out_bounds[r+1]) and computes the
+ *   entries entry_order[entry_bounds[r] .. entry_bounds[r+1]), listed by
+ *   increasing output index, entries of one output in batch order.
+ * The cuts balance entry counts as far as whole output groups allow.
+ * ylist (batchCount non-negative ints), entry_order (batchCount),
+ * entry_bounds and out_bounds (nranks + 1 each) are host arrays;
+ * out_bounds[0] = 0, out_bounds[nranks] = 1 + max(ylist).
+ * KRON_ERROR_INVALID_VALUE for a negative index or count, nranks < 1 or a
+ * missing array; KRON_ERROR_ALLOC if host memory runs out.
+ * ---------------------------------------------------------------------- */
+int kron_owner_partition(int batchCount, int const ylist[], int nranks, int entry_order[],
+                         int entry_bounds[], int out_bounds[]);
+
+/* ------------------------------------------------------------------------
  * Repeated application with a fixed operand (no reference counterpart): an
  * iterative solver applies the same kron(A_1..A_d) to a new X every
  * iteration.  kron_l2_persist_async keeps [ptr, ptr + bytes) -- typically A

@@ -82,6 +82,7 @@ def _sig(lib):
     S["kron_test_live_allocs"] = []
     S["kron_build_pointers_async"] = [_i, _i, _vp, C.c_longlong, _vp, _vp, C.c_longlong, _vp,
                                       _vp, C.c_longlong, _vp, _vp, _vp, _vp, _vp]
+    S["kron_owner_partition"] = [_i, _vp, _i, _vp, _vp, _vp]
     S["kron_l2_persist_async"] = [_vp, _sz, _vp]
     S["kron_l2_persist_reset"] = [_vp]
     S["kron_autotune"] = [_i, _i, _i, _i, _vp, _vp, _vp, _vp]
