@@ -106,15 +106,20 @@ def _problem():
 
 
 def _oracle(entries, ylist, xlist, alist, Apool, X, Y):
+    """The entries in list order: one oracle thread, so entries that share
+    an output add up in that order (bit-reproducible)."""
     import oracle
 
     if len(entries) == 0:
         return
+    old = oracle.num_threads()
+    oracle.set_threads(1)
     ap = [Apool.ctypes.data + 8 * N * N * int(alist[D * k + l]) for k in entries
           for l in range(D)]
     oracle.kronmult_general(D, [N] * D, [N] * D, ap, [N] * D,
                             [X.ctypes.data + 8 * L * int(xlist[k]) for k in entries],
                             [Y.ctypes.data + 8 * L * int(ylist[k]) for k in entries])
+    oracle.set_threads(old)
 
 
 def _free_port():
