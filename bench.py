@@ -720,10 +720,17 @@ class XbatchedBig(Workload):
         Yb.zero_()
         kb.kronmult_batched(d, n, Ab, self.dX, Yb, Wb)
         y64 = Yb.clone()
-        ms_sp = timeit(lambda: kb.kronmult_batched_split(d, n, Ab, self.dX, Yb, Wb))
-        Yb.zero_()
-        kb.kronmult_batched_split(d, n, Ab, self.dX, Yb, Wb)
-        torch.cuda.synchronize()
+        # split on the CUDA cores (two-phase launches), forced through the
+        # tuning table: the built-in choice at d = 6, n = 8 is the
+        # tensor-core form below
+        kb.tune_set(d, n, "split", "large")
+        try:
+            ms_sp = timeit(lambda: kb.kronmult_batched_split(d, n, Ab, self.dX, Yb, Wb))
+            Yb.zero_()
+            kb.kronmult_batched_split(d, n, Ab, self.dX, Yb, Wb)
+            torch.cuda.synchronize()
+        finally:
+            kb.tune_set(d, n, "split", None)
         out["batched_fp64"] = {"ms_per_step": round(ms64, 4),
                                "value": round(flop / ms64 / 1e6, 2), "unit": "GFLOP/s",
                                "layout": f"batched, the same {B} entries, distinct outputs"}
@@ -731,7 +738,22 @@ class XbatchedBig(Workload):
             "ms_per_step": round(ms_sp, 4), "value": round(flop / ms_sp / 1e6, 2),
             "unit": "GFLOP/s", "max_rel_err_vs_fp64": max_rel_err(torch, Yb, y64),
             "arithmetic": "hi+lo FP32 parts of A and X, three cross products with compensated "
-                          "FP32 sums, CUDA cores (no TF32/BF16 tensor-core split)"}
+                          "FP32 sums, CUDA cores"}
+        # the same split call with the 8x8 mode products as exact BF16 slice
+        # products on the tcgen05 tensor cores (the built-in choice)
+        kb.tune_set(d, n, "split", "split_tc")
+        try:
+            ms_tc = timeit(lambda: kb.kronmult_batched_split(d, n, Ab, self.dX, Yb, Wb))
+            Yb.zero_()
+            kb.kronmult_batched_split(d, n, Ab, self.dX, Yb, Wb)
+            torch.cuda.synchronize()
+            out["batched_split_tc"] = {
+                "ms_per_step": round(ms_tc, 4), "value": round(flop / ms_tc / 1e6, 2),
+                "unit": "GFLOP/s", "max_rel_err_vs_fp64": max_rel_err(torch, Yb, y64),
+                "arithmetic": "six 8-bit slices of A and X per mode product, BF16 tcgen05.mma "
+                              "with FP32 accumulators (exact), FP64 reconstruction"}
+        finally:
+            kb.tune_set(d, n, "split", None)
         del Ab, Yb, Wb, y_tc
         torch.cuda.empty_cache()
         return out
@@ -1064,7 +1086,12 @@ def run_ours(args, world, rank, local):
     kb.lib()
     wl = make_workload(args.config, args.precision, args.entries, args.n)
     tuned = None
-    if args.autotune and hasattr(wl, "n") and hasattr(wl, "d"):
+    if args.variant and hasattr(wl, "n") and hasattr(wl, "d"):
+        # force one kernel form for this square (d, n, precision)
+        name, _, q = args.variant.partition(":")
+        kb.tune_set(wl.d, wl.n, getattr(wl, "precision", "f64"), name, int(q or 0))
+        tuned = f"{name}:{int(q or 0)} (forced)"
+    elif args.autotune and hasattr(wl, "n") and hasattr(wl, "d"):
         # pick the kernel variant for this square (d, n, precision) before
         # anything is timed
         prec = getattr(wl, "precision", "f64")
@@ -1286,7 +1313,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=3)
     ap.add_argument("--n", type=int, default=int(os.environ.get("KRON_BENCH_N", "6")),
-                    choices=[4, 6], help="config 3: factor size (default 6)")
+                    choices=[4, 6, 8],
+                    help="config 3: factor size (default 6; 8 for profiling cases with --entries)")
     ap.add_argument("--mode", default="atomic", choices=["atomic", "segmented"])
     ap.add_argument("--precision", default="f64", choices=["f64", "f32", "split"])
     ap.add_argument("--cpu-sample", type=int, default=1 << 30)
@@ -1297,6 +1325,9 @@ def main():
                     help="skip the comparison legs of configs 3, 4 and 5")
     ap.add_argument("--no-check", action="store_true",
                     help="skip the error check against the reference's output")
+    ap.add_argument("--variant", default="",
+                    help="force a kernel form through the tuning table: name[:param] "
+                         "(mma8, pipe, sq, gen, big, large, slab, split_tc)")
     ap.add_argument("--autotune", action="store_true",
                     help="run the library's autotuner for the workload's shape first")
     ap.add_argument("--entries", type=int, default=0,

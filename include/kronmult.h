@@ -372,6 +372,11 @@ int kron_l2_persist_reset(kron_stream_t stream);
  *                       KRON_BIG_NO_L2_HINTS to drop the L2 cache policies
  *                       that keep W resident (a comparison form)
  *   KRON_VARIANT_LARGE  two-phase launches through the workspace W
+ *   KRON_VARIANT_SPLIT_TC  split precision (KRON_PREC_SPLIT) for d = 6,
+ *                       n = 8 in the batched layout with W: the two phases'
+ *                       8x8 mode products as exact BF16 slice products on the
+ *                       tcgen05 tensor cores, FP32 accumulators, FP64
+ *                       reconstruction (param unused)
  *   KRON_VARIANT_SLAB   slab-cluster kernel for d = 6, n = 6 (FP64 and
  *                       FP32): one cluster of 12 blocks per entry, each
  *                       block holding half of one n^5 slab, no workspace;
@@ -404,6 +409,7 @@ int kron_l2_persist_reset(kron_stream_t stream);
 #define KRON_VARIANT_BIG 5
 #define KRON_VARIANT_LARGE 6
 #define KRON_VARIANT_SLAB 7
+#define KRON_VARIANT_SPLIT_TC 8
 #define KRON_BIG_CUDA_CORES 256
 #define KRON_BIG_SMEM_W 512
 #define KRON_BIG_NO_L2_HINTS 1024

@@ -239,7 +239,8 @@ def l2_persist_reset(stream=None):
 
 # ---------------------------------------------------------------- autotuner
 PRECISIONS = {"f64": 0, "f32": 1, "split": 2}
-VARIANTS = {1: "mma8", 2: "pipe", 3: "sq", 4: "gen", 5: "big", 6: "large", 7: "slab"}
+VARIANTS = {1: "mma8", 2: "pipe", 3: "sq", 4: "gen", 5: "big", 6: "large", 7: "slab",
+            8: "split_tc"}
 # "big" param bit: FP64 d = 6, n = 8 on CUDA-core FMAs instead of tensor cores
 BIG_CUDA_CORES = 256
 # "big" param bit: keep the intermediate in the cluster's shared memory

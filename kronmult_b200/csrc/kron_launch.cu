@@ -507,6 +507,9 @@ int launch_variant(Params p, int prec, const Workspace &ws, int variant, int par
   case VAR_SLAB:
     return slab_supported(p, prec) ? launch_slab(p, prec, param, stream)
                                     : KRON_ERROR_NOT_SUPPORTED;
+  case VAR_SPLIT_TC:
+    return splittc_supported(p, prec, ws) ? launch_splittc(p, ws, stream)
+                                          : KRON_ERROR_NOT_SUPPORTED;
   case VAR_LARGE:
     if (prec == PREC_F32)
       return launch_large_t<float>(prec, p, ws, stream);
@@ -534,13 +537,17 @@ int launch_kron(Params p, int prec, const Workspace &ws, cudaStream_t stream)
       return rc;
   }
   // default order: the specialised kernels, then the general ones
-  static const int order[] = {VAR_MMA8, VAR_PIPE, VAR_SLAB, VAR_SQ, VAR_GEN, VAR_BIG, VAR_LARGE};
+  // (VAR_SPLIT_TC: split precision at d = 6, n = 8 on the tcgen05 tensor
+  // cores, 3.6 ms for 256 entries against 7.5 ms for the CUDA-core split)
+  static const int order[] = {VAR_MMA8, VAR_PIPE,     VAR_SLAB, VAR_SQ,
+                              VAR_GEN,  VAR_BIG,      VAR_SPLIT_TC, VAR_LARGE};
   for (int v : order)
   {
     if ((v == VAR_MMA8 && std::getenv("KRON_DISABLE_MMA8")) ||
         (v == VAR_PIPE && std::getenv("KRON_DISABLE_PIPE")) ||
         (v == VAR_SLAB && std::getenv("KRON_DISABLE_SLAB")) ||
-        (v == VAR_BIG && std::getenv("KRON_DISABLE_BIG")))
+        (v == VAR_BIG && std::getenv("KRON_DISABLE_BIG")) ||
+        (v == VAR_SPLIT_TC && std::getenv("KRON_DISABLE_SPLIT_TC")))
       continue;
     const int rc = launch_variant(p, prec, ws, v, 0, stream);
     if (rc != KRON_ERROR_NOT_SUPPORTED)

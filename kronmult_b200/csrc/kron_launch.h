@@ -51,6 +51,12 @@ long long drain_limit();
 bool big_supported(const Params &p, int prec);
 int launch_big(Params p, const Workspace &ws, int prec, int cluster, cudaStream_t stream);
 
+// Split precision (FP64 data, exact BF16 slice products on the tcgen05 tensor
+// cores) for square d = 6, n = 8 in the batched layout with a workspace W
+// (kron_splittc.cu).
+bool splittc_supported(const Params &p, int prec, const Workspace &ws);
+int launch_splittc(Params p, const Workspace &ws, cudaStream_t stream);
+
 // Kernel variants the launcher chooses among (values of KRON_VARIANT_* in
 // kronmult.h).
 enum Variant : int
@@ -65,6 +71,7 @@ enum Variant : int
                  // | KRON_BIG_SMEM_W (FP64 n = 6: W in the cluster's shared memory)
   VAR_LARGE = 6, // two-phase launches through the workspace (param unused)
   VAR_SLAB  = 7, // slab-cluster kernel, no workspace; param: KRON_SLAB_NO_ROTATE
+  VAR_SPLIT_TC = 8, // split precision d = 6, n = 8 on the tcgen05 tensor cores
 };
 
 // Work items of a launch (launch_kron does this before any variant).

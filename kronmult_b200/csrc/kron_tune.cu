@@ -42,7 +42,7 @@ struct TuneChoice
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneChoice> g_tune;
 
-bool valid_variant(int v) { return v >= VAR_MMA8 && v <= VAR_SLAB; }
+bool valid_variant(int v) { return v >= VAR_MMA8 && v <= VAR_SPLIT_TC; }
 
 } // namespace
 
@@ -69,7 +69,7 @@ static_assert(KRON_PREC_F64 == PREC_F64 && KRON_PREC_F32 == PREC_F32 &&
 static_assert(KRON_VARIANT_MMA8 == VAR_MMA8 && KRON_VARIANT_PIPE == VAR_PIPE &&
                   KRON_VARIANT_SQ == VAR_SQ && KRON_VARIANT_GEN == VAR_GEN &&
                   KRON_VARIANT_BIG == VAR_BIG && KRON_VARIANT_LARGE == VAR_LARGE &&
-                  KRON_VARIANT_SLAB == VAR_SLAB,
+                  KRON_VARIANT_SLAB == VAR_SLAB && KRON_VARIANT_SPLIT_TC == VAR_SPLIT_TC,
               "variant codes");
 
 extern "C" int kron_tune_set(int d, int n, int precision, int variant, int param)
