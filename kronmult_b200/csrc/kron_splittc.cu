@@ -124,9 +124,38 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16])
 
 __device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// BF16 bits of an integer-valued q with |q| <= 256 (exact: the FP32 value's
-// upper half)
-__device__ __forceinline__ uint32_t bf16_bits(double q) { return __float_as_uint((float)q) >> 16; }
+// The conversions below stay off the XU pipe (which a first version, with
+// rint and FP64 <-> FP32 casts, kept 52% busy): rounding by adding and
+// subtracting 1.5 * 2^52, BF16 bits and FP64 values put together from the
+// operands' bit fields with integer operations.
+
+// nearest integer (ties to even) of |v| < 2^51 by two FP64 adds
+__device__ __forceinline__ double round_int(double v)
+{
+  return __dadd_rn(__dadd_rn(v, 6755399441055744.0), -6755399441055744.0);
+}
+
+// BF16 bits of an integer-valued q with |q| <= 256, from q's FP64 fields:
+// the exponent rebiased from 1023 to 127, the mantissa's top 7 bits (exact:
+// q has at most 8 significant bits); zero of either sign gives +0
+__device__ __forceinline__ uint32_t bf16_bits(double q)
+{
+  const uint32_t h = (uint32_t)__double2hiint(q);
+  const uint32_t b = (((h >> 13) & 0x3FFFFu) - (896u << 7)) | ((h >> 16) & 0x8000u);
+  return (h & 0x7FFFFFFFu) ? b : 0u;
+}
+
+// FP64 value of an integer-valued FP32 d with |d| < 2^22: the integer
+// through the FP32 add of 1.5 * 2^23, then the FP64 subtraction of
+// 2^52 + 2^31 from the double whose low word is that integer + 2^31
+__device__ __forceinline__ double int_float_to_double(float d)
+{
+  const int i = __float_as_int(__fadd_rn(d, 12582912.0f)) - 0x4B400000;
+  return __dsub_rn(__hiloint2double(0x43300000, i ^ (int)0x80000000), 4503601774854144.0);
+}
+
+// 2^e for -1000 < e < 1000 from its bit fields (no ldexp)
+__device__ __forceinline__ double pow2(int e) { return __hiloint2double((1023 + e) << 20, 0); }
 
 // Cut v[0..7] (one fibre or one factor row) into NSL slices after scaling by
 // 2^-E; writes slice s's eight BF16 values as 16 bytes at dst + s * sstride.
@@ -137,13 +166,23 @@ __device__ __forceinline__ int slice8(const double (&v)[8], unsigned char *dst, 
 #pragma unroll
   for (int k = 0; k < 8; k++)
     mx = fmax(mx, fabs(v[k]));
+  // mx = m 2^E with m in [0.5, 1): E from the exponent field when mx is
+  // normal, frexp otherwise
   int E = 0;
   if (mx > 0.0)
-    frexp(mx, &E);
+  {
+    const int ex = (__double2hiint(mx) >> 20) & 0x7FF;
+    if (ex > 0 && ex < 0x7FF)
+      E = ex - 1022;
+    else
+      frexp(mx, &E);
+  }
+  const bool fast = E > -1000 && E < 1000;
+  const double sc = fast ? pow2(-E) : 0.0;
   double u[8];
 #pragma unroll
   for (int k = 0; k < 8; k++)
-    u[k] = ldexp(v[k], -E); // |u| < 1
+    u[k] = fast ? v[k] * sc : ldexp(v[k], -E); // |u| < 1, exact
 #pragma unroll
   for (int s = 0; s < NSL; s++)
   {
@@ -151,7 +190,7 @@ __device__ __forceinline__ int slice8(const double (&v)[8], unsigned char *dst, 
 #pragma unroll
     for (int k = 0; k < 8; k += 2)
     {
-      const double q0 = rint(u[k] * 256.0), q1 = rint(u[k + 1] * 256.0);
+      const double q0 = round_int(u[k] * 256.0), q1 = round_int(u[k + 1] * 256.0);
       u[k]            = u[k] * 256.0 - q0; // exact
       u[k + 1]        = u[k + 1] * 256.0 - q1;
       w[k / 2]        = bf16_bits(q0) | (bf16_bits(q1) << 16);
@@ -231,11 +270,12 @@ __device__ bool tile_modes(unsigned char *smem, double *buf, TcState &st, long l
 #pragma unroll
     for (int i = 0; i < 8; i++)
     {
-      double acc = (double)D[8 * (NSL - 1) + i];
+      double acc = int_float_to_double(D[8 * (NSL - 1) + i]);
 #pragma unroll
       for (int w = NSL - 2; w >= 0; --w)
-        acc = fma(acc, 0.00390625, (double)D[8 * w + i]); // 2^-8
-      buf[base + i * stride] = ldexp(acc, E + fexp[f * 8 + i] - 16);
+        acc = fma(acc, 0.00390625, int_float_to_double(D[8 * w + i])); // 2^-8
+      const int e = E + fexp[f * 8 + i] - 16;
+      buf[base + i * stride] = (e > -1000 && e < 1000) ? acc * pow2(e) : ldexp(acc, e);
     }
     // accumulator reads done before the next MMAs overwrite it; the tile's
     // outputs in place before the next mode reads other fibres
