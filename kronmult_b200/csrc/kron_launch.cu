@@ -508,7 +508,7 @@ int launch_variant(Params p, int prec, const Workspace &ws, int variant, int par
     return slab_supported(p, prec) ? launch_slab(p, prec, param, stream)
                                     : KRON_ERROR_NOT_SUPPORTED;
   case VAR_SPLIT_TC:
-    return splittc_supported(p, prec, ws) ? launch_splittc(p, ws, stream)
+    return splittc_supported(p, prec) ? launch_splittc(p, ws, stream)
                                           : KRON_ERROR_NOT_SUPPORTED;
   case VAR_LARGE:
     if (prec == PREC_F32)

@@ -54,7 +54,7 @@ int launch_big(Params p, const Workspace &ws, int prec, int cluster, cudaStream_
 // Split precision (FP64 data, exact BF16 slice products on the tcgen05 tensor
 // cores) for square d = 6, n = 8 in the batched layout with a workspace W
 // (kron_splittc.cu).
-bool splittc_supported(const Params &p, int prec, const Workspace &ws);
+bool splittc_supported(const Params &p, int prec);
 int launch_splittc(Params p, const Workspace &ws, cudaStream_t stream);
 
 // Kernel variants the launcher chooses among (values of KRON_VARIANT_* in

@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(TC_THREADS, 4)
 
 } // namespace
 
-bool splittc_supported(const Params &p, int prec, const Workspace &ws)
+bool splittc_supported(const Params &p, int prec)
 {
   if (prec != PREC_SPLIT || p.d != 6 || p.layout != LAYOUT_BATCHED || p.seg_off ||
       (p.accum != ACC_DISTINCT && p.accum != ACC_ATOMIC))

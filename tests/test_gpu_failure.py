@@ -3,7 +3,8 @@ faults, traps or hangs a GPU.
 
 - Wait time-out: a bound of one poll (kron_set_wait_limit) makes the
   pipelined kernel (d = 6, n = 4) and the slab-cluster kernel (d = 6, n = 6)
-  give up on their first asynchronous copy.  The copies still land (the
+  give up on their first asynchronous copy, and the tensor-core split
+  kernels (d = 6, n = 8) on their first MMA commit.  The copies still land (the
   drain keeps the full bound) and the kernels return.  The status word then
   reads 1, and the next call with the default bound is clean and correct.
 - Allocation failure: an injected device-allocation failure
@@ -64,6 +65,36 @@ def test_wait_timeout_then_clean(gpu_lib, n, variant, batch):
     dY = dev(Y0)
     kb.kronmult_batched(d, n, dA, dX, dY, None)
     assert rel_err(host(dY), Yref) <= 1e-13
+    assert lib.kron_device_status(1) == 0
+
+
+def test_wait_timeout_tensor_core_split_then_clean(gpu_lib):
+    """The tcgen05 split kernels (d = 6, n = 8): with a one-poll bound the
+    wait for the first commit of the MMAs runs out; each block waits for its
+    MMAs with the full drain bound, frees its tensor memory and leaves."""
+    import torch
+
+    lib = kb.lib()
+    d, n, batch = 6, 8, 2
+    L = n ** d
+    rng = np.random.default_rng(708)
+    A = rng.standard_normal(n * n * d * batch) / np.sqrt(n)
+    X = rng.uniform(-1, 1, L * batch)
+    Y0 = rng.uniform(-1, 1, L * batch)
+    kb.tune_set(d, n, "split", "split_tc")
+    dA, dX = dev(A), dev(X)
+    W = torch.empty(L * batch, dtype=torch.float64, device="cuda")
+    assert lib.kron_device_status(1) in (0, 1)
+    assert lib.kron_set_wait_limit(1) == 0
+    kb.kronmult_batched_split(d, n, dA, dX, dev(Y0), W)
+    torch.cuda.synchronize()
+    assert lib.kron_set_wait_limit(0) == 0
+    assert lib.kron_device_status(1) == 1, "the one-poll wait should have run out"
+    Yref = Y0.copy()
+    oracle.kronmult_batched(d, n, A, X, Yref)
+    dY = dev(Y0)
+    kb.kronmult_batched_split(d, n, dA, dX, dY, W)
+    assert rel_err(host(dY), Yref) <= 1e-12
     assert lib.kron_device_status(1) == 0
 
 
