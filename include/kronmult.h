@@ -385,7 +385,13 @@ int kron_l2_persist_reset(kron_stream_t stream);
  *                       KRON_SLAB_NO_ROTATE -- no lane rotation in its first
  *                       FP64 pass (which keeps that pass free of bank
  *                       conflicts); KRON_SLAB_PLAIN_Y -- distinct outputs
- *                       added by loads and stores instead of L2 atomics
+ *                       added by loads and stores instead of L2 atomics;
+ *                       KRON_SLAB_NO_SIDE -- no side kernel: by default,
+ *                       for FP64 batches of 512 entries or more with a
+ *                       workspace W, a share of the entries runs
+ *                       concurrently on the cluster two-phase kernel (a
+ *                       library-owned second stream, joined by events) on
+ *                       the SMs the 12-block clusters leave idle
  * kron_autotune times every variant that runs (d, n, precision) on a
  * synthetic batched problem of up to batchCount entries (capped at 1 GiB),
  * records the fastest for that key and returns it (outputs may be NULL).
@@ -416,6 +422,7 @@ int kron_l2_persist_reset(kron_stream_t stream);
 #define KRON_SLAB_NO_ROTATE 1
 #define KRON_SLAB_WHOLE 2
 #define KRON_SLAB_PLAIN_Y 4
+#define KRON_SLAB_NO_SIDE 8
 
 int kron_autotune(int d, int n, int precision, int batchCount, int *variant, int *param,
                   double *best_us, kron_stream_t stream);

@@ -254,6 +254,8 @@ SLAB_NO_ROTATE = 1
 SLAB_WHOLE = 2
 # "slab" param bit: distinct outputs by loads and stores (comparison form)
 SLAB_PLAIN_Y = 4
+# "slab" param bit: no side kernel on the SMs the slab clusters leave idle
+SLAB_NO_SIDE = 8
 
 
 def autotune(d, n, precision="f64", batch=1024, stream=None):

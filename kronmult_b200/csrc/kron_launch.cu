@@ -467,6 +467,114 @@ int sq_entries_max(int prec, int d, int n, bool merge)
   return std::max(1, std::min(256 / ki.GS, (int)(device_info().max_smem_optin / ki.group_bytes)));
 }
 
+// ---- slab-cluster kernel with a side kernel on the SMs it leaves idle ----
+//
+// The slab kernel's clusters of 12 blocks fill whole GPCs only so far: on
+// B200 its 21 resident clusters hold 126 of the 148 SMs.  When the caller
+// passes a workspace, a share of the entries goes to the cluster two-phase
+// kernel (clusters of 2) on a second stream, whose blocks take the idle SMs
+// while the slab kernel runs.  The share gives each idle SM SIDE_RATE of a
+// slab SM's entries (measured for 4096 entries of d = 6, n = 6: 1.59 ms
+// alone; 1.40 ms with 13% of the entries on the side, 1.43 ms with 10%;
+// 1.60 ms with 16%, where the side kernel finishes last -- hence the
+// cautious rate).  The two launches are joined by events, also inside a
+// stream capture (the side stream is created by the first call outside
+// one; a call under capture before that runs the slab kernel alone).
+namespace {
+
+constexpr double SIDE_RATE         = 0.75;
+constexpr long long SIDE_MIN_ENTRIES = 512;
+
+struct SideRes
+{
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+std::mutex g_side_mu;
+SideRes g_side[64];
+
+// the side stream and events of the current device; created outside
+// capture only
+bool side_resources(bool capturing, SideRes *&out)
+{
+  const int dev = device_info().device;
+  if (dev < 0 || dev >= 64)
+    return false;
+  SideRes &r = g_side[dev];
+  if (!r.stream)
+  {
+    if (capturing)
+      return false;
+    if (cudaStreamCreateWithFlags(&r.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r.fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r.join, cudaEventDisableTiming) != cudaSuccess)
+    {
+      cudaGetLastError();
+      if (r.stream)
+        cudaStreamDestroy(r.stream);
+      if (r.fork)
+        cudaEventDestroy(r.fork);
+      r = SideRes{};
+      return false;
+    }
+  }
+  out = &r;
+  return true;
+}
+
+bool side_workspace(const Params &p, const Workspace &ws, long long L)
+{
+  if (p.layout == LAYOUT_BATCHED)
+    return ws.W && ws.wstride >= L;
+  if (ws.pW)
+    return ws.pw_elems >= L && ws.npW >= 1;
+  return ws.W && ws.Wbytes >= (size_t)L * sizeof(double);
+}
+
+} // namespace
+
+int launch_slab_side(Params p, int prec, const Workspace &ws, int flags, cudaStream_t stream)
+{
+  const long long work = p.eend - p.ebase;
+  long long L = 1;
+  for (int l = 0; l < p.d; l++)
+    L *= p.n[l];
+  int used = 0;
+  const int sms = device_info().sms;
+  if (prec != PREC_F64 || (flags & KRON_SLAB_NO_SIDE) || work < SIDE_MIN_ENTRIES ||
+      !big_supported(p, prec) || !side_workspace(p, ws, L) ||
+      slab_sms_used(p.n[0], prec, flags, &used) != KRON_SUCCESS || sms - used < 2)
+    return launch_slab(p, prec, flags, stream);
+  const int idle       = sms - used;
+  const long long side = (long long)((double)work * (idle * SIDE_RATE) / (used + idle * SIDE_RATE));
+  if (side < 1)
+    return launch_slab(p, prec, flags, stream);
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  // an error here (the legacy stream while another stream captures) counts
+  // as capturing
+  const bool capturing =
+      cudaStreamIsCapturing(stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone;
+  cudaGetLastError();
+  std::lock_guard<std::mutex> lock(g_side_mu);
+  SideRes *r = nullptr;
+  if (!side_resources(capturing, r))
+    return launch_slab(p, prec, flags, stream);
+  Params ps = p, pb = p;
+  ps.eend  = (int)(p.eend - side);
+  pb.ebase = ps.eend;
+  if (cudaEventRecord(r->fork, stream) != cudaSuccess ||
+      cudaStreamWaitEvent(r->stream, r->fork, 0) != cudaSuccess)
+    return KRON_ERROR_LAUNCH;
+  // the slab kernel first, so that its clusters take their SMs before the
+  // side kernel's blocks are placed
+  const int rc1 = launch_slab(ps, prec, flags, stream);
+  const int rc2 = launch_big(pb, ws, prec, 0, r->stream);
+  if (cudaEventRecord(r->join, r->stream) != cudaSuccess ||
+      cudaStreamWaitEvent(stream, r->join, 0) != cudaSuccess)
+    return KRON_ERROR_LAUNCH;
+  return rc1 != KRON_SUCCESS ? rc1 : rc2;
+}
+
 int launch_variant(Params p, int prec, const Workspace &ws, int variant, int param,
                    cudaStream_t stream)
 {
@@ -505,7 +613,7 @@ int launch_variant(Params p, int prec, const Workspace &ws, int variant, int par
     return big_supported(p, prec) ? launch_big(p, ws, prec, param, stream)
                                   : KRON_ERROR_NOT_SUPPORTED;
   case VAR_SLAB:
-    return slab_supported(p, prec) ? launch_slab(p, prec, param, stream)
+    return slab_supported(p, prec) ? launch_slab_side(p, prec, ws, param, stream)
                                     : KRON_ERROR_NOT_SUPPORTED;
   case VAR_SPLIT_TC:
     return splittc_supported(p, prec) ? launch_splittc(p, ws, stream)

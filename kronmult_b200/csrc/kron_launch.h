@@ -38,6 +38,13 @@ int launch_pipe(Params p, int prec, cudaStream_t stream);
 // memory whose n slabs of n^5 elements fit (kron_slab.cu).
 bool slab_supported(const Params &p, int prec);
 int launch_slab(Params p, int prec, int flags, cudaStream_t stream);
+// SMs that the slab kernel's resident clusters occupy (the cluster shape can
+// leave some SMs of each GPC without a whole cluster).
+int slab_sms_used(int n, int prec, int flags, int *used);
+// The slab kernel plus a side kernel (cluster two-phase, second stream) on
+// the SMs its clusters leave idle, when p and the workspace allow
+// (kron_launch.cu).
+int launch_slab_side(Params p, int prec, const Workspace &ws, int flags, cudaStream_t stream);
 
 // Device status word (kron_status.cu): its device address for kernel
 // arguments, the poll bound of mbarrier waits (kron_set_wait_limit), and the

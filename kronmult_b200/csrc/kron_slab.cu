@@ -543,14 +543,16 @@ __global__ void __maxnreg__((SlabShape<T, N, H>::MAXREG))
         mbar_wait_bounded(&bars[s], (phase >> s) & 1, drain);
 }
 
+// Launch configuration of the slab kernel and the clusters the device runs
+// at once (ncl), with the blocks each SM holds (per_sm).
 template <typename T, int N, int H>
-int launch_slab_t(Params p, int flags, cudaStream_t stream)
+int slab_config_t(cudaLaunchConfig_t &cfg, cudaLaunchAttribute *attr, int &ncl, int &per_sm)
 {
   using S        = SlabShape<T, N, H>;
   const void *fn = reinterpret_cast<const void *>(&kron_slab_kernel<T, N, H>);
   if (S::SMEM > (size_t)device_info().max_smem_optin)
     return KRON_ERROR_NOT_SUPPORTED;
-  int per_sm = 1;
+  per_sm = 1;
   if (cached_occupancy(fn, S::THREADS, S::SMEM, &per_sm) != KRON_SUCCESS)
     return KRON_ERROR_LAUNCH;
   if (S::CS > 8)
@@ -572,31 +574,58 @@ int launch_slab_t(Params p, int flags, cudaStream_t stream)
       nonportable_set[dev] = true;
     }
   }
-  cudaLaunchConfig_t cfg = {};
-  cudaLaunchAttribute attr[1];
+  cfg                      = cudaLaunchConfig_t{};
   attr[0].id               = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = S::CS;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.blockDim             = dim3(S::THREADS);
   cfg.dynamicSmemBytes     = S::SMEM;
-  cfg.stream               = stream;
   cfg.attrs                = attr;
   cfg.numAttrs             = 1;
   cfg.gridDim              = dim3((device_info().sms / S::CS) * S::CS);
-  int ncl                  = 0;
+  ncl                      = 0;
   if (cudaOccupancyMaxActiveClusters(&ncl, fn, &cfg) != cudaSuccess || ncl < 1)
   {
     cudaGetLastError();
     return KRON_ERROR_NOT_SUPPORTED;
   }
+  return KRON_SUCCESS;
+}
+
+template <typename T, int N, int H>
+int launch_slab_t(Params p, int flags, cudaStream_t stream)
+{
+  const void *fn = reinterpret_cast<const void *>(&kron_slab_kernel<T, N, H>);
+  cudaLaunchConfig_t cfg;
+  cudaLaunchAttribute attr[1];
+  int ncl = 0, per_sm = 1;
+  const int rc = slab_config_t<T, N, H>(cfg, attr, ncl, per_sm);
+  if (rc != KRON_SUCCESS)
+    return rc;
+  using S      = SlabShape<T, N, H>;
   ncl          = (int)std::min<long long>((long long)ncl, p.eend - p.ebase);
   cfg.gridDim  = dim3(ncl * S::CS);
+  cfg.stream   = stream;
   int *status  = device_status_ptr();
   long long sp = wait_limit();
   long long dr = drain_limit();
   void *args[] = {&p, &status, &sp, &dr, &flags};
   return cudaLaunchKernelExC(&cfg, fn, args) == cudaSuccess ? KRON_SUCCESS : KRON_ERROR_LAUNCH;
+}
+
+template <typename T, int N, int H>
+int slab_sms_t(int &used)
+{
+  cudaLaunchConfig_t cfg;
+  cudaLaunchAttribute attr[1];
+  int ncl = 0, per_sm = 1;
+  const int rc = slab_config_t<T, N, H>(cfg, attr, ncl, per_sm);
+  if (rc != KRON_SUCCESS)
+    return rc;
+  using S = SlabShape<T, N, H>;
+  used    = std::min(device_info().sms, (ncl * S::CS + per_sm - 1) / std::max(1, per_sm));
+  return KRON_SUCCESS;
 }
 
 } // namespace
@@ -611,6 +640,16 @@ bool slab_supported(const Params &p, int prec)
     if (p.m[l] != n || p.n[l] != n)
       return false;
   return n == 6;
+}
+
+int slab_sms_used(int n, int prec, int flags, int *used)
+{
+  *used = 0;
+  if (n != 6)
+    return KRON_ERROR_NOT_SUPPORTED;
+  if (flags & KRON_SLAB_WHOLE)
+    return prec == PREC_F32 ? slab_sms_t<float, 6, 1>(*used) : slab_sms_t<double, 6, 1>(*used);
+  return prec == PREC_F32 ? slab_sms_t<float, 6, 2>(*used) : slab_sms_t<double, 6, 2>(*used);
 }
 
 int launch_slab(Params p, int prec, int flags, cudaStream_t stream)

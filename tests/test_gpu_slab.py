@@ -9,7 +9,9 @@ Covers every path of the kernel:
   xbatched factors with lda > n);
 - results added into y at any alignment (y shifted by one element);
 - outputs that alias (pbatched);
-- FP32 and FP64.
+- FP32 and FP64;
+- the side kernel that takes a share of large FP64 batches on the SMs the
+  clusters leave idle (batched and aliasing pbatched, with W).
 FP64 bar: normwise relative error <= 1e-13; FP32 <= 1e-5 against the FP64
 oracle."""
 import numpy as np
@@ -132,3 +134,46 @@ def test_slab_matches_two_phase(gpu_lib):
         kb.kronmult_batched(D, N, dA, dX, dY, W)
         out[v] = host(dY)
     assert rel_err(out["slab"], out["big"]) <= 1e-14
+
+
+@pytest.mark.parametrize("forced", [None, 0, kb.SLAB_NO_SIDE, kb.SLAB_WHOLE])
+def test_slab_with_side_kernel(gpu_lib, forced):
+    """FP64 batches of 512 entries or more with a workspace: a share of the
+    entries runs concurrently on the cluster two-phase kernel (second
+    stream) on the SMs the slab clusters leave idle.  Batched with W, the
+    default and forced forms, and the opt-out bit."""
+    import torch
+
+    batch = 700
+    if forced is not None:
+        kb.tune_set(D, N, "f64", "slab", forced)
+    A, X, Y0 = _inputs(batch, 6006)
+    Yref = Y0.copy()
+    oracle.kronmult_batched(D, N, A, X, Yref)
+    dY = dev(Y0)
+    W = torch.empty(L * batch, dtype=torch.float64, device="cuda")
+    kb.kronmult_batched(D, N, dev(A), dev(X), dY, W)
+    assert rel_err(host(dY), Yref) <= TOL["f64"]
+    assert gpu_lib.kron_device_status(1) == 0
+
+
+def test_slab_with_side_kernel_aliasing_pbatched(gpu_lib):
+    """pbatched with outputs that alias (600 entries onto 150 columns) and a
+    W pointer per entry: both kernels add into shared columns atomically."""
+    import torch
+
+    batch, ny = 600, 150
+    A, X, Y0 = _inputs(batch, 6007, ny)
+    yl = np.random.default_rng(6008).integers(0, ny, size=batch)
+    Yref = Y0.copy()
+    oracle.kronmult_general(D, [N] * D, [N] * D,
+                            [A.ctypes.data + 8 * N * N * (D * k + l) for k in range(batch)
+                             for l in range(D)],
+                            [N] * D, [X.ctypes.data + 8 * L * k for k in range(batch)],
+                            [Yref.ctypes.data + 8 * L * int(j) for j in yl])
+    dX, dY = dev(X), dev(Y0)
+    W = torch.empty(L * batch, dtype=torch.float64, device="cuda")
+    kb.kronmult_pbatched(D, N, dev(A), ptrs(dX, L * np.arange(batch)), ptrs(dY, L * yl),
+                         pW=ptrs(W, L * np.arange(batch)))
+    assert rel_err(host(dY), Yref) <= TOL["f64"]
+    assert gpu_lib.kron_device_status(1) == 0
