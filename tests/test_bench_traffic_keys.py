@@ -17,7 +17,7 @@ def _args(config, precision="f64", mode="atomic", entries=0, n=6):
     (1, "f64", 6, "cfg1"), (2, "f64", 6, "cfg2"), (3, "f64", 4, "cfg3"),
     (3, "f32", 4, "cfg3-f32"), (3, "split", 4, "cfg3-split"),
     (3, "f64", 6, "cfg3-n6"), (3, "f32", 6, "cfg3-f32-n6"),
-    (4, "f64", 6, "cfg4"), (5, "f64", 6, "cfg5"),
+    (4, "f64", 6, "cfg4"), (5, "f64", 6, "cfg5"), (6, "f64", 6, "cfg6"),
 ])
 def test_every_workload_has_a_traffic_line(config, precision, n, key):
     args = _args(config, precision, n=n)
